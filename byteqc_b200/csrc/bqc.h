@@ -1,0 +1,56 @@
+// Internal declarations shared by the CUDA translation units of libbyteqc_b200.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include "../../include/byteqc_b200.h"
+
+#define BQC_LMAX 3          // s, p, d, f
+#define BQC_NCART_MAX 10
+
+// Everything a J/K kernel launch reads.  Device pointers unless noted.
+struct JKArgs {
+    const int *pair_bra;      // shell i of each pair        (bas_pair2bra)
+    const int *pair_ket;      // shell j of each pair        (bas_pair2ket)
+    const double *a12, *e12, *x12, *y12, *z12;  // primitive-pair data
+    const double *bas_x, *bas_y, *bas_z;        // shell centres
+    const int *ao_loc;        // Cartesian AO offsets of the sorted, decontracted basis
+    const double *pair_q;     // Schwarz factor of each pair, or NULL (no screening)
+    const double *dm_cond;    // [nbas*nbas] max |D| over each shell block, or NULL
+    const double *dm;         // [n_dm][nao][nao]
+    double *vj, *vk;          // [n_dm][nao][nao] accumulated (NULL disables)
+    int nao, nbas, n_dm;
+    double tol;               // drop quartets with q_ij q_kl max|D| < tol
+    int *status;              // device error word (0 = ok), may be NULL
+    const double *rys;        // Rys coefficient table (bqc_rys_table())
+};
+
+// One rectangular (or triangular, when diag) block of the quartet space.
+struct JKTask {
+    int a0, na;        // bra pairs [a0, a0 + na) (global pair indices)
+    int b0, nb;        // ket pairs
+    int pa0, pb0;      // primitive-pair offset of the first bra / ket pair
+    int nprim_a, nprim_b;  // primitive pairs per bra / ket pair
+    int diag;          // bra and ket lists are the same: keep a >= b only
+    int skip_lower;    // reference rule: skip global pair index a < b
+    // Optional tile pruning.  Tiles are rows x columns of 16 x 16 quartets,
+    // rows over the a list (or the b list when rows_are_b).  With
+    // tile_prefix (device, nrows + 1 entries) row r holds the columns
+    // [0, tile_prefix[r+1] - tile_prefix[r]) and block x maps to the tile
+    // with tile_prefix[r] <= x < tile_prefix[r+1]; without it the grid is
+    // the full rectangle.
+    const int *tile_prefix;
+    int nrows;
+    int ntiles;        // number of tiles (blocks) when tile_prefix is set
+    int rows_are_b;
+};
+
+// device address of the Rys coefficient table on the current device (rys_table.cu)
+const double *bqc_rys_table();
+
+// launchers (jk_dispatch.cu, schwarz.cu)
+int bqc_launch_jk(int li, int lj, int lk, int ll, const JKArgs &args, const JKTask &task,
+                  int fp32, cudaStream_t stream);
+int bqc_launch_dm_cond(const double *dm, int n_dm, int nao, const int *ao_loc, int nbas,
+                       double *dm_cond, cudaStream_t stream);
+int bqc_launch_schwarz(int li, int lj, const JKArgs &args, int p0, int np, int pa0, int nprim,
+                       double diag_fac, double *q_out, cudaStream_t stream);

@@ -1,0 +1,297 @@
+// C ABI of libbyteqc_b200: the reference-compatible GINT* entry points and the
+// native whole-build BQC* entry points (declared in include/byteqc_b200.h).
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <vector>
+#include "bqc.h"
+
+#define ATM_SLOTS 6
+#define BAS_SLOTS 8
+#define PTR_COORD 1
+#define ATOM_OF 0
+#define ANG_OF 1
+#define NPRIM_OF 2
+#define PTR_EXP 5
+#define PTR_COEFF 6
+
+// normalisation constant of a Cartesian s or p function (the remaining
+// spherical-harmonic normalisation of l >= 2 sits in the cart2sph matrix)
+static double fac_sp(int l) {
+    return l == 0 ? 0.282094791773878143 : (l == 1 ? 0.488602511902919921 : 1.0);
+}
+
+extern "C" {
+
+// Class table and primitive-pair block, as cuobc/lib/gint/pair_data.c:30-142
+// defines them: one class per (l_bra, l_ket, nprim_bra * nprim_ket) group of
+// consecutive pairs; per primitive pair a12 = ai + aj,
+// e12 = fac_sp(li) fac_sp(lj) ci cj exp(-ai aj |AB|^2 / a12) (times diag_fac
+// when ish == jsh) and the Gaussian product centre.
+void GINTinit_basis_prod_cpu(BasisProdCache **pbp, double diag_fac, double *bas_coords,
+                             int *bas_pair2shls, int *bas_pairs_locs, int ncptype, int *atm,
+                             int natm, int *bas, int nbas, double *env) {
+    (void)natm;
+    BasisProdCache *bp = (BasisProdCache *)calloc(1, sizeof(BasisProdCache));
+    *pbp = bp;
+    bp->nbas = nbas;
+    bp->ncptype = ncptype;
+    bp->bas_pairs_locs = bas_pairs_locs;
+    bp->bas_pair2shls = bas_pair2shls;
+    const int npairs_tot = bas_pairs_locs[ncptype];
+    const int *bra = bas_pair2shls, *ket = bas_pair2shls + npairs_tot;
+    bp->cptype = (ContractionProdType *)malloc(sizeof(ContractionProdType) * (ncptype > 0 ? ncptype : 1));
+    bp->primitive_pairs_locs = (int *)malloc(sizeof(int) * (ncptype + 1));
+    bp->primitive_pairs_locs[0] = 0;
+    for (int c = 0; c < ncptype; c++) {
+        int p0 = bas_pairs_locs[c], np = bas_pairs_locs[c + 1] - p0;
+        ContractionProdType *t = bp->cptype + c;
+        if (np > 0) {
+            int ish = bra[p0], jsh = ket[p0];
+            t->l_bra = bas[ish * BAS_SLOTS + ANG_OF];
+            t->l_ket = bas[jsh * BAS_SLOTS + ANG_OF];
+            t->nprim_12 = bas[ish * BAS_SLOTS + NPRIM_OF] * bas[jsh * BAS_SLOTS + NPRIM_OF];
+        } else {
+            t->l_bra = t->l_ket = 0;
+            t->nprim_12 = 1;
+        }
+        t->npairs = np;
+        bp->primitive_pairs_locs[c + 1] = bp->primitive_pairs_locs[c] + np * t->nprim_12;
+    }
+    const int nprim_tot = bp->primitive_pairs_locs[ncptype];
+    double *aexyz = (double *)malloc(sizeof(double) * 5 * (nprim_tot > 0 ? nprim_tot : 1));
+    bp->aexyz = aexyz;
+    double *a12 = aexyz, *e12 = a12 + nprim_tot, *x12 = e12 + nprim_tot;
+    double *y12 = x12 + nprim_tot, *z12 = y12 + nprim_tot;
+    int off = 0;
+    for (int p = 0; p < npairs_tot; p++) {
+        int ish = bra[p], jsh = ket[p];
+        const int *bi = bas + ish * BAS_SLOTS, *bj = bas + jsh * BAS_SLOTS;
+        const double *ri = env + atm[bi[ATOM_OF] * ATM_SLOTS + PTR_COORD];
+        const double *rj = env + atm[bj[ATOM_OF] * ATM_SLOTS + PTR_COORD];
+        const double *ai = env + bi[PTR_EXP], *aj = env + bj[PTR_EXP];
+        const double *ci = env + bi[PTR_COEFF], *cj = env + bj[PTR_COEFF];
+        double norm = fac_sp(bi[ANG_OF]) * fac_sp(bj[ANG_OF]);
+        if (ish == jsh) norm *= diag_fac;
+        double dx = ri[0] - rj[0], dy = ri[1] - rj[1], dz = ri[2] - rj[2];
+        double r2 = dx * dx + dy * dy + dz * dz;
+        for (int ip = 0; ip < bi[NPRIM_OF]; ip++) {
+            for (int jp = 0; jp < bj[NPRIM_OF]; jp++, off++) {
+                double aij = ai[ip] + aj[jp];
+                a12[off] = aij;
+                e12[off] = norm * ci[ip] * cj[jp] * exp(-r2 * ai[ip] * aj[jp] / aij);
+                x12[off] = (ai[ip] * ri[0] + aj[jp] * rj[0]) / aij;
+                y12[off] = (ai[ip] * ri[1] + aj[jp] * rj[1]) / aij;
+                z12[off] = (ai[ip] * ri[2] + aj[jp] * rj[2]) / aij;
+            }
+        }
+    }
+    for (int ib = 0; ib < nbas; ib++) {
+        const double *r = env + atm[bas[ib * BAS_SLOTS + ATOM_OF] * ATM_SLOTS + PTR_COORD];
+        bas_coords[ib] = r[0];
+        bas_coords[ib + nbas] = r[1];
+        bas_coords[ib + 2 * nbas] = r[2];
+    }
+}
+
+void GINTinit_basis_prod_gpu(BasisProdCache **pbpin, BasisProdCache **pbp, int *ao_loc,
+                             double *bas_coords, double *aexyz, int *bas_pair2shls) {
+    BasisProdCache *bp = (BasisProdCache *)malloc(sizeof(BasisProdCache));
+    memcpy(bp, *pbpin, sizeof(BasisProdCache));
+    *pbp = bp;
+    // the device copy shares the host class table; only the cpu cache owns it
+    bp->aexyz = NULL;
+    bp->ao_loc = ao_loc;
+    bp->bas_coords = bas_coords;
+    int npairs = bp->bas_pairs_locs[bp->ncptype];
+    int nprim = bp->primitive_pairs_locs[bp->ncptype];
+    bp->a12 = aexyz;
+    bp->e12 = aexyz + nprim;
+    bp->x12 = aexyz + 2 * (size_t)nprim;
+    bp->y12 = aexyz + 3 * (size_t)nprim;
+    bp->z12 = aexyz + 4 * (size_t)nprim;
+    bp->bas_pair2bra = bas_pair2shls;
+    bp->bas_pair2ket = bas_pair2shls + npairs;
+}
+
+void GINTdel_basis_prod(BasisProdCache **pbp) {
+    BasisProdCache *bp = *pbp;
+    if (bp == NULL) return;
+    if (bp->aexyz != NULL) {
+        // host cache: owns the class table and the primitive-pair block
+        free(bp->cptype);
+        free(bp->primitive_pairs_locs);
+        free(bp->aexyz);
+    }
+    free(bp);
+    *pbp = NULL;
+}
+
+static JKArgs make_args(const BasisProdCache *bp, double *vj, double *vk, const double *dm,
+                        int nao, int n_dm) {
+    JKArgs a;
+    memset(&a, 0, sizeof(a));
+    a.pair_bra = bp->bas_pair2bra;
+    a.pair_ket = bp->bas_pair2ket;
+    a.a12 = bp->a12;
+    a.e12 = bp->e12;
+    a.x12 = bp->x12;
+    a.y12 = bp->y12;
+    a.z12 = bp->z12;
+    a.bas_x = bp->bas_coords;
+    a.bas_y = bp->bas_coords + bp->nbas;
+    a.bas_z = bp->bas_coords + 2 * bp->nbas;
+    a.ao_loc = bp->ao_loc;
+    a.dm = dm;
+    a.vj = vj;
+    a.vk = vk;
+    a.nao = nao;
+    a.nbas = bp->nbas;
+    a.n_dm = n_dm;
+    a.rys = bqc_rys_table();
+    return a;
+}
+
+int GINTbuild_jk(BasisProdCache *bpcache, double *vj, double *vk, double *dm, int nao, int n_dm,
+                 int *bins_locs_ij, int *bins_locs_kl, int nbins, int cp_ij_id, int cp_kl_id,
+                 cudaStream_t stream) {
+    const ContractionProdType *cij = bpcache->cptype + cp_ij_id;
+    const ContractionProdType *ckl = bpcache->cptype + cp_kl_id;
+    int L = cij->l_bra + cij->l_ket + ckl->l_bra + ckl->l_ket;
+    if (L / 2 + 1 >= 12) return 2;
+    if (cij->l_bra > BQC_LMAX || ckl->l_bra > BQC_LMAX) return 2;
+    JKArgs args = make_args(bpcache, vj, vk, dm, nao, n_dm);
+    for (int kl_bin = 0; kl_bin < nbins; kl_bin++) {
+        int kl0 = bins_locs_kl[kl_bin], kl1 = bins_locs_kl[kl_bin + 1];
+        if (kl1 <= kl0) continue;
+        int ij0 = bins_locs_ij[0], ij1 = bins_locs_ij[nbins - kl_bin];
+        if (ij1 <= ij0) continue;
+        JKTask t;
+        memset(&t, 0, sizeof(t));
+        t.a0 = bpcache->bas_pairs_locs[cp_ij_id] + ij0;
+        t.na = ij1 - ij0;
+        t.b0 = bpcache->bas_pairs_locs[cp_kl_id] + kl0;
+        t.nb = kl1 - kl0;
+        t.pa0 = bpcache->primitive_pairs_locs[cp_ij_id] + ij0 * cij->nprim_12;
+        t.pb0 = bpcache->primitive_pairs_locs[cp_kl_id] + kl0 * ckl->nprim_12;
+        t.nprim_a = cij->nprim_12;
+        t.nprim_b = ckl->nprim_12;
+        t.diag = cp_ij_id == cp_kl_id;
+        t.skip_lower = 1;
+        int err = bqc_launch_jk(cij->l_bra, cij->l_ket, ckl->l_bra, ckl->l_ket, args, t, 0, stream);
+        if (err) return err;
+    }
+    return 0;
+}
+
+// Tile rows of one class-pair task: row r (16 pairs of the a list, q sorted
+// descending) keeps the columns whose first (largest) q_b satisfies
+// q_a[16 r] q_b[16 c] dm_max >= tol; on a diagonal task also c <= r.
+static int tile_rows(const double *qa, int na, const double *qb, int nb, double dm_max, double tol,
+                     int diag, std::vector<int> &prefix) {
+    int nta = (na + 15) / 16, ntb = (nb + 15) / 16;
+    prefix.push_back(0);
+    int base = (int)prefix.size() - 1;
+    for (int r = 0; r < nta; r++) {
+        double qr = qa[16 * r] * dm_max;
+        int lo = 0, hi = ntb;   // count of leading columns with qb[16 c] * qr >= tol
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            if (qb[16 * mid] * qr >= tol) lo = mid + 1; else hi = mid;
+        }
+        int n = lo;
+        if (diag && n > r + 1) n = r + 1;
+        prefix.push_back(prefix.back() + n);
+    }
+    return prefix.back() - prefix[base];
+}
+
+int BQCbuild_jk(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
+                const double *dm_cond, double dm_max, double *vj, double *vk, const double *dm,
+                int nao, int n_dm, double tol, double fp32_below, int *status_dev,
+                cudaStream_t stream) {
+    (void)fp32_below;
+    JKArgs args = make_args(bp, vj, vk, dm, nao, n_dm);
+    args.pair_q = pair_q;
+    args.dm_cond = dm_cond;
+    args.tol = tol;
+    args.status = status_dev;
+    if (dm_cond == nullptr) dm_max = 1.0;
+    std::vector<JKTask> tasks;
+    std::vector<int> shape;   // (li, lj, lk, ll) per task
+    std::vector<int> prefix;
+    std::vector<size_t> prefix_off;
+    for (int cij = 0; cij < bp->ncptype; cij++) {
+        const ContractionProdType *tij = bp->cptype + cij;
+        if (tij->npairs == 0) continue;
+        for (int ckl = 0; ckl <= cij; ckl++) {
+            const ContractionProdType *tkl = bp->cptype + ckl;
+            if (tkl->npairs == 0) continue;
+            if (tij->l_bra > BQC_LMAX || tkl->l_bra > BQC_LMAX) return 2;
+            JKTask t;
+            memset(&t, 0, sizeof(t));
+            t.a0 = bp->bas_pairs_locs[cij];
+            t.na = tij->npairs;
+            t.b0 = bp->bas_pairs_locs[ckl];
+            t.nb = tkl->npairs;
+            t.pa0 = bp->primitive_pairs_locs[cij];
+            t.pb0 = bp->primitive_pairs_locs[ckl];
+            t.nprim_a = tij->nprim_12;
+            t.nprim_b = tkl->nprim_12;
+            t.diag = cij == ckl;
+            t.skip_lower = 1;
+            if (pair_q_host != nullptr) {
+                size_t off = prefix.size();
+                int n = tile_rows(pair_q_host + t.a0, t.na, pair_q_host + t.b0, t.nb, dm_max, tol,
+                                  t.diag, prefix);
+                if (n == 0) {
+                    prefix.resize(off);
+                    continue;
+                }
+                t.nrows = (t.na + 15) / 16;
+                t.ntiles = n;
+                prefix_off.push_back(off);
+            }
+            tasks.push_back(t);
+            shape.push_back(tij->l_bra);
+            shape.push_back(tij->l_ket);
+            shape.push_back(tkl->l_bra);
+            shape.push_back(tkl->l_ket);
+        }
+    }
+    int *d_prefix = nullptr;
+    if (pair_q_host != nullptr && !prefix.empty()) {
+        if (cudaMallocAsync((void **)&d_prefix, sizeof(int) * prefix.size(), stream) != cudaSuccess)
+            return 1;
+        cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int) * prefix.size(),
+                        cudaMemcpyHostToDevice, stream);
+    }
+    int err = 0;
+    for (size_t i = 0; i < tasks.size() && !err; i++) {
+        if (d_prefix) tasks[i].tile_prefix = d_prefix + prefix_off[i];
+        err = bqc_launch_jk(shape[4 * i], shape[4 * i + 1], shape[4 * i + 2], shape[4 * i + 3],
+                            args, tasks[i], 0, stream);
+    }
+    if (d_prefix) cudaFreeAsync(d_prefix, stream);
+    return err;
+}
+
+int BQCdm_cond(const double *dm, int n_dm, int nao, const int *ao_loc, int nbas, double *dm_cond,
+               cudaStream_t stream) {
+    return bqc_launch_dm_cond(dm, n_dm, nao, ao_loc, nbas, dm_cond, stream);
+}
+
+int BQCschwarz(const BasisProdCache *bp, int cp, double diag_fac, double *q_out,
+               cudaStream_t stream) {
+    const ContractionProdType *t = bp->cptype + cp;
+    if (t->npairs == 0) return 0;
+    if (t->l_bra > BQC_LMAX) return 2;
+    JKArgs args = make_args(bp, NULL, NULL, NULL, 0, 0);
+    return bqc_launch_schwarz(t->l_bra, t->l_ket, args, bp->bas_pairs_locs[cp], t->npairs,
+                              bp->primitive_pairs_locs[cp], t->nprim_12, diag_fac, q_out, stream);
+}
+
+const char *BQCversion(void) { return "byteqc_b200 0.1 sm_100a"; }
+
+}  // extern "C"

@@ -1,0 +1,658 @@
+// J/K kernels of the direct-SCF engine for sm_100a.
+//
+// One template instance per shell-quartet class (LI LJ | LK LL).  A launch
+// covers one block of the quartet space of a class pair: bra pairs
+// [a0, a0 + na) x ket pairs [b0, b0 + nb), cut into 16 x 16 tiles.  Each CTA
+// takes one tile, screens its 256 quartets on the device against
+// q_ij q_kl max|D| >= tol (the six density blocks a quartet touches), packs
+// the survivors into a shared-memory list and evaluates them:
+//
+// * jk_small: one thread per quartet for classes with at most SMALL_NF
+//   Cartesian components; the 2D integrals and the contracted quartet block
+//   live in registers and the six J/K targets are digested from registers.
+// * jk_group: TPQ = nfi * nfj * NSPLIT threads per quartet; thread
+//   (fi, fj, chunk) owns the ket components (fk in its chunk, all fl) of bra
+//   component (fi, fj).  Per primitive quartet the group evaluates the Rys
+//   roots and the per-root 2D tables (VRR + HRR) cooperatively into shared
+//   memory, then every thread accumulates its components.  Digestion: J_ij is
+//   a thread-local dot product; the K targets and J_kl are reduced through
+//   shared memory before one FP64 atomic per output element.
+//
+// The per-quartet factors follow the reference (cuobc/lib/gvhf/g2e.cu:1021-1028,
+// cuobc/lib/gint/pair_data.c:135-139): 1/2 when the bra and ket pairs are the
+// same pair (a == b), and the 1/2 of a diagonal shell pair carried in e12.
+#pragma once
+#include <stdio.h>
+#include "jk_device.cuh"
+
+namespace bqc {
+
+constexpr int TILE = 16;
+constexpr int SMALL_NF = 36;
+constexpr double TWO_PI_2P5 = 34.986836655249725693;  // 2 pi^(5/2)
+
+// ---------------------------------------------------------------------------
+// tile screening: returns false (uniformly) if the tile holds no quartet
+__device__ __forceinline__ double dmax6(const double *__restrict__ dmc, int nbas, int i, int j,
+                                        int k, int l) {
+    double m = fmax(__ldg(dmc + i * nbas + j), __ldg(dmc + k * nbas + l));
+    m = fmax(m, __ldg(dmc + i * nbas + k));
+    m = fmax(m, __ldg(dmc + i * nbas + l));
+    m = fmax(m, __ldg(dmc + j * nbas + k));
+    return fmax(m, __ldg(dmc + j * nbas + l));
+}
+
+__device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, int *s_list,
+                                            int *s_count, int &a_begin, int &b_begin,
+                                            int &count) {
+    int r, c;
+    if (T.tile_prefix != nullptr) {
+        // largest r with tile_prefix[r] <= blockIdx.x
+        int lo = 0, hi = T.nrows - 1;
+        const int x = blockIdx.x;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (__ldg(T.tile_prefix + mid) <= x) lo = mid; else hi = mid - 1;
+        }
+        r = lo;
+        c = x - __ldg(T.tile_prefix + r);
+    } else {
+        int ncols = ((T.rows_are_b ? T.na : T.nb) + TILE - 1) / TILE;
+        r = blockIdx.x / ncols;
+        c = blockIdx.x % ncols;
+    }
+    int ta = T.rows_are_b ? c : r, tb = T.rows_are_b ? r : c;
+    a_begin = T.a0 + ta * TILE;
+    b_begin = T.b0 + tb * TILE;
+    int a_end = min(T.a0 + T.na, a_begin + TILE);
+    int b_end = min(T.b0 + T.nb, b_begin + TILE);
+    if (T.diag && b_begin > a_end - 1) return false;
+    if (threadIdx.x == 0) *s_count = 0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < TILE * TILE; e += blockDim.x) {
+        int a = a_begin + e / TILE, b = b_begin + e % TILE;
+        bool keep = a < a_end && b < b_end && (!T.diag || a >= b);
+        if (keep && A.pair_q != nullptr) {
+            double bound = __ldg(A.pair_q + a) * __ldg(A.pair_q + b);
+            if (A.dm_cond != nullptr) {
+                int i = __ldg(A.pair_bra + a), j = __ldg(A.pair_ket + a);
+                int k = __ldg(A.pair_bra + b), l = __ldg(A.pair_ket + b);
+                bound *= dmax6(A.dm_cond, A.nbas, i, j, k, l);
+            }
+            keep = bound >= A.tol;
+        }
+        if (keep) {
+            int idx = atomicAdd(s_count, 1);
+            s_list[idx] = ((a - a_begin) << 16) | (b - b_begin);
+        }
+    }
+    __syncthreads();
+    count = *s_count;
+    return count > 0;
+}
+
+struct Quartet {
+    int a, b, ish, jsh, ksh, lsh, i0, j0, k0, l0;
+    double A[3], B[3], C[3], D[3];
+    double fac;
+};
+
+__device__ __forceinline__ void load_quartet(const JKArgs &A, int a, int b, Quartet &q) {
+    q.a = a;
+    q.b = b;
+    q.ish = __ldg(A.pair_bra + a);
+    q.jsh = __ldg(A.pair_ket + a);
+    q.ksh = __ldg(A.pair_bra + b);
+    q.lsh = __ldg(A.pair_ket + b);
+    q.i0 = __ldg(A.ao_loc + q.ish);
+    q.j0 = __ldg(A.ao_loc + q.jsh);
+    q.k0 = __ldg(A.ao_loc + q.ksh);
+    q.l0 = __ldg(A.ao_loc + q.lsh);
+    const int sh[4] = {q.ish, q.jsh, q.ksh, q.lsh};
+    double *dst[4] = {q.A, q.B, q.C, q.D};
+#pragma unroll
+    for (int s = 0; s < 4; s++) {
+        dst[s][0] = __ldg(A.bas_x + sh[s]);
+        dst[s][1] = __ldg(A.bas_y + sh[s]);
+        dst[s][2] = __ldg(A.bas_z + sh[s]);
+    }
+    q.fac = (a == b) ? 0.5 * TWO_PI_2P5 : TWO_PI_2P5;
+}
+
+// primitive-pair quantities of one primitive quartet
+struct PrimQuartet {
+    double p, q, inv_pq, x, pref;
+    double PA[3], QC[3], PQ[3];
+};
+
+__device__ __forceinline__ void load_prim(const JKArgs &A, const Quartet &Q, int pi, int pk,
+                                          PrimQuartet &P) {
+    double aij = __ldg(A.a12 + pi), eij = __ldg(A.e12 + pi);
+    double akl = __ldg(A.a12 + pk), ekl = __ldg(A.e12 + pk);
+    double Pc[3] = {__ldg(A.x12 + pi), __ldg(A.y12 + pi), __ldg(A.z12 + pi)};
+    double Qc[3] = {__ldg(A.x12 + pk), __ldg(A.y12 + pk), __ldg(A.z12 + pk)};
+    P.p = aij;
+    P.q = akl;
+    double s = aij + akl;
+    P.inv_pq = 1.0 / s;
+    double rr = 0;
+#pragma unroll
+    for (int d = 0; d < 3; d++) {
+        P.PA[d] = Pc[d] - Q.A[d];
+        P.QC[d] = Qc[d] - Q.C[d];
+        P.PQ[d] = Pc[d] - Qc[d];
+        rr += P.PQ[d] * P.PQ[d];
+    }
+    P.x = aij * akl * P.inv_pq * rr;
+    P.pref = Q.fac * eij * ekl / (aij * akl * sqrt(s));
+}
+
+// ---------------------------------------------------------------------------
+// thread-per-quartet kernel
+template <int LI, int LJ, int LK, int LL, typename F>
+__global__ void __launch_bounds__(256) jk_small(JKArgs A, JKTask T) {
+    constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = ncart(LK), NFL = ncart(LL);
+    constexpr int NF = NFI * NFJ * NFK * NFL;
+    constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
+    constexpr int GSZ = (LI + 1) * (LJ + 1) * (LK + 1) * (LL + 1);
+    __shared__ int s_list[TILE * TILE];
+    __shared__ int s_count;
+    int a_begin, b_begin, count;
+    if (!tile_screen(A, T, s_list, &s_count, a_begin, b_begin, count)) return;
+
+    for (int it = threadIdx.x; it < count; it += blockDim.x) {
+        int e = s_list[it];
+        Quartet Q;
+        load_quartet(A, a_begin + (e >> 16), b_begin + (e & 0xffff), Q);
+        F AB[3], CD[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            AB[d] = F(Q.A[d] - Q.B[d]);
+            CD[d] = F(Q.C[d] - Q.D[d]);
+        }
+        F acc[NF];
+#pragma unroll
+        for (int n = 0; n < NF; n++) acc[n] = F(0);
+        int pa = T.pa0 + (Q.a - T.a0) * T.nprim_a;
+        int pb = T.pb0 + (Q.b - T.b0) * T.nprim_b;
+        for (int ip = 0; ip < T.nprim_a; ip++) {
+            for (int kp = 0; kp < T.nprim_b; kp++) {
+                PrimQuartet P;
+                load_prim(A, Q, pa + ip, pb + kp, P);
+                double rt[NR], wt[NR];
+                rys_roots<NR>(A.rys, P.x, rt, wt);
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    RootCoef c = root_coef(rt[r], P.p, P.q, P.inv_pq);
+                    F g[3][GSZ];
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        F seed = (d == 2) ? F(wt[r] * P.pref) : F(1);
+                        gen_2d<LI, LJ, LK, LL, F>(seed, F(P.PA[d] - c.qs * P.PQ[d]),
+                                                  F(P.QC[d] + c.ps * P.PQ[d]), F(c.b00),
+                                                  F(c.b10), F(c.b01), AB[d], CD[d], g[d]);
+                    }
+#pragma unroll
+                    for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                    for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                    for (int fk = 0; fk < NFK; fk++)
+#pragma unroll
+                    for (int fl = 0; fl < NFL; fl++) {
+                        constexpr int SJ = (LK + 1) * (LL + 1), SI = (LJ + 1) * SJ;
+                        int ix = cart_pow(LI, fi, 0) * SI + cart_pow(LJ, fj, 0) * SJ +
+                                 cart_pow(LK, fk, 0) * (LL + 1) + cart_pow(LL, fl, 0);
+                        int iy = cart_pow(LI, fi, 1) * SI + cart_pow(LJ, fj, 1) * SJ +
+                                 cart_pow(LK, fk, 1) * (LL + 1) + cart_pow(LL, fl, 1);
+                        int iz = cart_pow(LI, fi, 2) * SI + cart_pow(LJ, fj, 2) * SJ +
+                                 cart_pow(LK, fk, 2) * (LL + 1) + cart_pow(LL, fl, 2);
+                        int n = ((fi * NFJ + fj) * NFK + fk) * NFL + fl;
+                        acc[n] += g[0][ix] * g[1][iy] * g[2][iz];
+                    }
+                }
+            }
+        }
+        // digestion (FP64)
+        const int nao = A.nao;
+        const size_t nn = (size_t)nao * nao;
+        for (int id = 0; id < A.n_dm; id++) {
+            const double *__restrict__ D = A.dm + id * nn;
+            if (A.vj != nullptr) {
+                double *VJ = A.vj + id * nn;
+                double dkl[NFK * NFL], dij[NFI * NFJ];
+#pragma unroll
+                for (int fk = 0; fk < NFK; fk++)
+#pragma unroll
+                    for (int fl = 0; fl < NFL; fl++)
+                        dkl[fk * NFL + fl] = __ldg(D + (size_t)(Q.k0 + fk) * nao + Q.l0 + fl);
+#pragma unroll
+                for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                    for (int fj = 0; fj < NFJ; fj++)
+                        dij[fi * NFJ + fj] = __ldg(D + (size_t)(Q.i0 + fi) * nao + Q.j0 + fj);
+#pragma unroll
+                for (int ij = 0; ij < NFI * NFJ; ij++) {
+                    double s = 0;
+#pragma unroll
+                    for (int kl = 0; kl < NFK * NFL; kl++) s += (double)acc[ij * NFK * NFL + kl] * dkl[kl];
+                    atomicAdd(VJ + (size_t)(Q.i0 + ij / NFJ) * nao + Q.j0 + ij % NFJ, s);
+                }
+#pragma unroll
+                for (int kl = 0; kl < NFK * NFL; kl++) {
+                    double s = 0;
+#pragma unroll
+                    for (int ij = 0; ij < NFI * NFJ; ij++) s += (double)acc[ij * NFK * NFL + kl] * dij[ij];
+                    atomicAdd(VJ + (size_t)(Q.k0 + kl / NFL) * nao + Q.l0 + kl % NFL, s);
+                }
+            }
+            if (A.vk != nullptr) {
+                double *VK = A.vk + id * nn;
+                double djl[NFJ][NFL], djk[NFJ][NFK], dil[NFI][NFL], dik[NFI][NFK];
+#pragma unroll
+                for (int fj = 0; fj < NFJ; fj++) {
+#pragma unroll
+                    for (int fl = 0; fl < NFL; fl++) djl[fj][fl] = __ldg(D + (size_t)(Q.j0 + fj) * nao + Q.l0 + fl);
+#pragma unroll
+                    for (int fk = 0; fk < NFK; fk++) djk[fj][fk] = __ldg(D + (size_t)(Q.j0 + fj) * nao + Q.k0 + fk);
+                }
+#pragma unroll
+                for (int fi = 0; fi < NFI; fi++) {
+#pragma unroll
+                    for (int fl = 0; fl < NFL; fl++) dil[fi][fl] = __ldg(D + (size_t)(Q.i0 + fi) * nao + Q.l0 + fl);
+#pragma unroll
+                    for (int fk = 0; fk < NFK; fk++) dik[fi][fk] = __ldg(D + (size_t)(Q.i0 + fi) * nao + Q.k0 + fk);
+                }
+#define ACC(fi, fj, fk, fl) ((double)acc[(((fi) * NFJ + (fj)) * NFK + (fk)) * NFL + (fl)])
+#pragma unroll
+                for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                    for (int fk = 0; fk < NFK; fk++) {
+                        double s = 0;
+#pragma unroll
+                        for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                            for (int fl = 0; fl < NFL; fl++) s += ACC(fi, fj, fk, fl) * djl[fj][fl];
+                        atomicAdd(VK + (size_t)(Q.i0 + fi) * nao + Q.k0 + fk, s);
+                    }
+#pragma unroll
+                for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                    for (int fl = 0; fl < NFL; fl++) {
+                        double s = 0;
+#pragma unroll
+                        for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                            for (int fk = 0; fk < NFK; fk++) s += ACC(fi, fj, fk, fl) * djk[fj][fk];
+                        atomicAdd(VK + (size_t)(Q.i0 + fi) * nao + Q.l0 + fl, s);
+                    }
+#pragma unroll
+                for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                    for (int fk = 0; fk < NFK; fk++) {
+                        double s = 0;
+#pragma unroll
+                        for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                            for (int fl = 0; fl < NFL; fl++) s += ACC(fi, fj, fk, fl) * dil[fi][fl];
+                        atomicAdd(VK + (size_t)(Q.j0 + fj) * nao + Q.k0 + fk, s);
+                    }
+#pragma unroll
+                for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                    for (int fl = 0; fl < NFL; fl++) {
+                        double s = 0;
+#pragma unroll
+                        for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                            for (int fk = 0; fk < NFK; fk++) s += ACC(fi, fj, fk, fl) * dik[fi][fk];
+                        atomicAdd(VK + (size_t)(Q.j0 + fj) * nao + Q.l0 + fl, s);
+                    }
+#undef ACC
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// group-per-quartet kernel
+template <int LI, int LJ, int LK, int LL, int NSPLIT>
+struct GroupCfg {
+    static constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = ncart(LK), NFL = ncart(LL);
+    static constexpr int NIJ = NFI * NFJ, NKL = NFK * NFL;
+    static constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
+    static constexpr int TPQ = NIJ * NSPLIT;
+    static constexpr int GSZ = (LI + 1) * (LJ + 1) * (LK + 1) * (LL + 1);
+    static constexpr int KLS = (LK + 1) * (LL + 1);
+    static constexpr int CK = cdiv(NFK, NSPLIT);
+    static constexpr int NACC = CK * NFL;
+    static constexpr int GBUF = 3 * NR * GSZ;
+    static constexpr int KSLOTS = 2 * NIJ * NFK + 2 * NIJ * NFL * NSPLIT;
+    static constexpr int RB = imax(GBUF, KSLOTS);
+    static constexpr int FKB = imax(1, RB / (NFL * NIJ));
+    static constexpr int DBUF = NIJ + NKL + NFI * NFK + NFI * NFL + NFJ * NFK + NFJ * NFL;
+    static constexpr int RW = 2 * NR;
+    static constexpr int PER_GROUP = RB + DBUF + RW;          // doubles
+    // groups per CTA: up to 256 threads and at most SMEM_BUDGET bytes of
+    // shared memory (two CTAs per SM)
+    static constexpr int SMEM_BUDGET = 112 * 1024;
+    static constexpr int NG = imax(1, imin(256 / TPQ, SMEM_BUDGET / (PER_GROUP * 8)));
+    static constexpr int NT = cdiv(NG * TPQ, 32) * 32;
+    static constexpr size_t SMEM = (size_t)NG * PER_GROUP * sizeof(double);
+};
+
+template <int LI, int LJ, int LK, int LL, int NSPLIT>
+__global__ void __launch_bounds__(GroupCfg<LI, LJ, LK, LL, NSPLIT>::NT)
+jk_group(JKArgs A, JKTask T) {
+    using C = GroupCfg<LI, LJ, LK, LL, NSPLIT>;
+    constexpr int NFI = C::NFI, NFJ = C::NFJ, NFK = C::NFK, NFL = C::NFL;
+    constexpr int NR = C::NR, TPQ = C::TPQ, NG = C::NG, GSZ = C::GSZ, CK = C::CK;
+    extern __shared__ double smem[];
+    __shared__ int s_list[TILE * TILE];
+    __shared__ int s_count;
+    int a_begin, b_begin, count;
+    if (!tile_screen(A, T, s_list, &s_count, a_begin, b_begin, count)) return;
+
+    const int g = threadIdx.x / TPQ;
+    const int lane = threadIdx.x % TPQ;
+    const bool in_group = g < NG;
+    double *gbuf = smem + (in_group ? g : 0) * C::PER_GROUP;   // RB: g tables / reduction
+    double *dbuf = gbuf + C::RB;                                // density blocks
+    double *rw = dbuf + C::DBUF;                                // roots, weights
+    double *Dij = dbuf, *Dkl = Dij + C::NIJ, *Dik = Dkl + C::NKL, *Dil = Dik + NFI * NFK;
+    double *Djk = Dil + NFI * NFL, *Djl = Djk + NFJ * NFK;
+
+    const int fij = lane / NSPLIT, chunk = lane % NSPLIT;
+    const int fi = fij / NFJ, fj = fij % NFJ;
+    const int ixb = cart_pow(LI, 0, 0);  // silence unused warnings of constexpr helpers
+    (void)ixb;
+    int pix = 0, piy = 0, piz = 0, pjx = 0, pjy = 0, pjz = 0;
+#pragma unroll
+    for (int c = 0; c < NFI; c++)
+        if (c == fi) { pix = cart_pow(LI, c, 0); piy = cart_pow(LI, c, 1); piz = cart_pow(LI, c, 2); }
+#pragma unroll
+    for (int c = 0; c < NFJ; c++)
+        if (c == fj) { pjx = cart_pow(LJ, c, 0); pjy = cart_pow(LJ, c, 1); pjz = cart_pow(LJ, c, 2); }
+    const int offx = (pix * (LJ + 1) + pjx) * C::KLS;
+    const int offy = GSZ * NR + (piy * (LJ + 1) + pjy) * C::KLS;
+    const int offz = 2 * GSZ * NR + (piz * (LJ + 1) + pjz) * C::KLS;
+
+    const int nrounds = (count + NG - 1) / NG;
+    for (int round = 0; round < nrounds; round++) {
+        const int item = round * NG + g;
+        const bool active = in_group && item < count;
+        Quartet Q;
+        double AB[3] = {0, 0, 0}, CD[3] = {0, 0, 0};
+        int pa = 0, pb = 0;
+        if (active) {
+            int e = s_list[item];
+            load_quartet(A, a_begin + (e >> 16), b_begin + (e & 0xffff), Q);
+#pragma unroll
+            for (int d = 0; d < 3; d++) {
+                AB[d] = Q.A[d] - Q.B[d];
+                CD[d] = Q.C[d] - Q.D[d];
+            }
+            pa = T.pa0 + (Q.a - T.a0) * T.nprim_a;
+            pb = T.pb0 + (Q.b - T.b0) * T.nprim_b;
+        }
+        double acc[C::NACC];
+#pragma unroll
+        for (int n = 0; n < C::NACC; n++) acc[n] = 0.0;
+
+        for (int ip = 0; ip < T.nprim_a; ip++) {
+            for (int kp = 0; kp < T.nprim_b; kp++) {
+                PrimQuartet P;
+                if (active) {
+                    load_prim(A, Q, pa + ip, pb + kp, P);
+                    for (int f = lane; f < 2 * NR; f += TPQ) rw[f] = rys_one<NR>(A.rys, P.x, f);
+                }
+                __syncthreads();
+                if (active) {
+                    for (int task = lane; task < 3 * NR; task += TPQ) {
+                        int r = task / 3, d = task % 3;
+                        RootCoef c = root_coef(rw[r], P.p, P.q, P.inv_pq);
+                        double seed = (d == 2) ? rw[NR + r] * P.pref : 1.0;
+                        gen_2d<LI, LJ, LK, LL, double>(seed, P.PA[d] - c.qs * P.PQ[d],
+                                                       P.QC[d] + c.ps * P.PQ[d], c.b00, c.b10,
+                                                       c.b01, AB[d], CD[d],
+                                                       gbuf + (d * NR + r) * GSZ);
+                    }
+                }
+                __syncthreads();
+                if (active && lane < TPQ) {
+#pragma unroll
+                    for (int r = 0; r < NR; r++) {
+                        const double *gx = gbuf + offx + r * GSZ;
+                        const double *gy = gbuf + offy + r * GSZ;
+                        const double *gz = gbuf + offz + r * GSZ;
+                        if constexpr (NSPLIT == 1) {
+                            double xs[C::KLS], ys[C::KLS], zs[C::KLS];
+#pragma unroll
+                            for (int u = 0; u < C::KLS; u++) {
+                                xs[u] = gx[u];
+                                ys[u] = gy[u];
+                                zs[u] = gz[u];
+                            }
+#pragma unroll
+                            for (int fk = 0; fk < NFK; fk++)
+#pragma unroll
+                            for (int fl = 0; fl < NFL; fl++) {
+                                int ux = cart_pow(LK, fk, 0) * (LL + 1) + cart_pow(LL, fl, 0);
+                                int uy = cart_pow(LK, fk, 1) * (LL + 1) + cart_pow(LL, fl, 1);
+                                int uz = cart_pow(LK, fk, 2) * (LL + 1) + cart_pow(LL, fl, 2);
+                                acc[fk * NFL + fl] = fma(xs[ux] * ys[uy], zs[uz], acc[fk * NFL + fl]);
+                            }
+                        } else {
+#pragma unroll
+                            for (int ck = 0; ck < CK; ck++) {
+                                int fk = chunk * CK + ck;
+                                if (fk < NFK) {
+                                    int kx = 0, ky = 0, kz = 0;
+#pragma unroll
+                                    for (int c = 0; c < NFK; c++)
+                                        if (c == fk) { kx = cart_pow(LK, c, 0); ky = cart_pow(LK, c, 1); kz = cart_pow(LK, c, 2); }
+                                    const double *rx = gx + kx * (LL + 1);
+                                    const double *ry = gy + ky * (LL + 1);
+                                    const double *rz = gz + kz * (LL + 1);
+#pragma unroll
+                                    for (int fl = 0; fl < NFL; fl++) {
+                                        acc[ck * NFL + fl] = fma(rx[cart_pow(LL, fl, 0)] * ry[cart_pow(LL, fl, 1)],
+                                                                 rz[cart_pow(LL, fl, 2)], acc[ck * NFL + fl]);
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+
+        // ---- digestion ----
+        const int nao = A.nao;
+        const size_t nn = (size_t)nao * nao;
+        for (int id = 0; id < A.n_dm; id++) {
+            const double *__restrict__ D = A.dm + id * nn;
+            if (active) {
+                for (int e = lane; e < C::DBUF; e += TPQ) {
+                    int r0 = 0, c0 = 0, nc = 1, o = e;
+                    if (o < C::NIJ) { r0 = Q.i0; c0 = Q.j0; nc = NFJ; }
+                    else if ((o -= C::NIJ) < C::NKL) { r0 = Q.k0; c0 = Q.l0; nc = NFL; }
+                    else if ((o -= C::NKL) < NFI * NFK) { r0 = Q.i0; c0 = Q.k0; nc = NFK; }
+                    else if ((o -= NFI * NFK) < NFI * NFL) { r0 = Q.i0; c0 = Q.l0; nc = NFL; }
+                    else if ((o -= NFI * NFL) < NFJ * NFK) { r0 = Q.j0; c0 = Q.k0; nc = NFK; }
+                    else { o -= NFJ * NFK; r0 = Q.j0; c0 = Q.l0; nc = NFL; }
+                    dbuf[e] = __ldg(D + (size_t)(r0 + o / nc) * nao + c0 + o % nc);
+                }
+            }
+            __syncthreads();
+            if (A.vj != nullptr && active) {
+                double s = 0;
+#pragma unroll
+                for (int ck = 0; ck < CK; ck++) {
+                    int fk = chunk * CK + ck;
+                    if (fk < NFK) {
+#pragma unroll
+                        for (int fl = 0; fl < NFL; fl++) s = fma(acc[ck * NFL + fl], Dkl[fk * NFL + fl], s);
+                    }
+                }
+                atomicAdd(A.vj + id * nn + (size_t)(Q.i0 + fi) * nao + Q.j0 + fj, s);
+            }
+            if (A.vk != nullptr) {
+                // K partials into shared slots
+                double *Sik = gbuf;                              // [fi][fk][fj]
+                double *Sjk = Sik + C::NIJ * NFK;                // [fj][fk][fi]
+                double *Sil = Sjk + C::NIJ * NFK;                // [fi][fl][fj][chunk]
+                double *Sjl = Sil + C::NIJ * NFL * NSPLIT;       // [fj][fl][fi][chunk]
+                if (active) {
+#pragma unroll
+                    for (int ck = 0; ck < CK; ck++) {
+                        int fk = chunk * CK + ck;
+                        if (fk < NFK) {
+                            double sik = 0, sjk = 0;
+#pragma unroll
+                            for (int fl = 0; fl < NFL; fl++) {
+                                sik = fma(acc[ck * NFL + fl], Djl[fj * NFL + fl], sik);
+                                sjk = fma(acc[ck * NFL + fl], Dil[fi * NFL + fl], sjk);
+                            }
+                            Sik[(fi * NFK + fk) * NFJ + fj] = sik;
+                            Sjk[(fj * NFK + fk) * NFI + fi] = sjk;
+                        }
+                    }
+#pragma unroll
+                    for (int fl = 0; fl < NFL; fl++) {
+                        double sil = 0, sjl = 0;
+#pragma unroll
+                        for (int ck = 0; ck < CK; ck++) {
+                            int fk = chunk * CK + ck;
+                            if (fk < NFK) {
+                                sil = fma(acc[ck * NFL + fl], Djk[fj * NFK + fk], sil);
+                                sjl = fma(acc[ck * NFL + fl], Dik[fi * NFK + fk], sjl);
+                            }
+                        }
+                        Sil[((fi * NFL + fl) * NFJ + fj) * NSPLIT + chunk] = sil;
+                        Sjl[((fj * NFL + fl) * NFI + fi) * NSPLIT + chunk] = sjl;
+                    }
+                }
+                __syncthreads();
+                if (active) {
+                    double *VK = A.vk + id * nn;
+                    constexpr int O1 = NFI * NFK, O2 = O1 + NFJ * NFK, O3 = O2 + NFI * NFL,
+                                  O4 = O3 + NFJ * NFL;
+                    for (int o = lane; o < O4; o += TPQ) {
+                        double s = 0;
+                        size_t dst;
+                        if (o < O1) {
+                            int a = o / NFK, k = o % NFK;
+                            for (int j = 0; j < NFJ; j++) s += Sik[(a * NFK + k) * NFJ + j];
+                            dst = (size_t)(Q.i0 + a) * nao + Q.k0 + k;
+                        } else if (o < O2) {
+                            int a = (o - O1) / NFK, k = (o - O1) % NFK;
+                            for (int i = 0; i < NFI; i++) s += Sjk[(a * NFK + k) * NFI + i];
+                            dst = (size_t)(Q.j0 + a) * nao + Q.k0 + k;
+                        } else if (o < O3) {
+                            int a = (o - O2) / NFL, l = (o - O2) % NFL;
+                            for (int j = 0; j < NFJ * NSPLIT; j++) s += Sil[(a * NFL + l) * NFJ * NSPLIT + j];
+                            dst = (size_t)(Q.i0 + a) * nao + Q.l0 + l;
+                        } else {
+                            int a = (o - O3) / NFL, l = (o - O3) % NFL;
+                            for (int i = 0; i < NFI * NSPLIT; i++) s += Sjl[(a * NFL + l) * NFI * NSPLIT + i];
+                            dst = (size_t)(Q.j0 + a) * nao + Q.l0 + l;
+                        }
+                        atomicAdd(VK + dst, s);
+                    }
+                }
+                __syncthreads();
+            }
+            if (A.vj != nullptr) {
+                double *VJ = A.vj + id * nn;
+                const double dij = active ? Dij[fi * NFJ + fj] : 0.0;
+                for (int fk0 = 0; fk0 < NFK; fk0 += C::FKB) {
+                    double *Sj = gbuf;   // [fk - fk0][fl][fij]
+                    if (active) {
+#pragma unroll
+                        for (int ck = 0; ck < CK; ck++) {
+                            int fk = chunk * CK + ck;
+                            if (fk >= fk0 && fk < fk0 + C::FKB && fk < NFK) {
+#pragma unroll
+                                for (int fl = 0; fl < NFL; fl++)
+                                    Sj[((fk - fk0) * NFL + fl) * C::NIJ + fij] = acc[ck * NFL + fl] * dij;
+                            }
+                        }
+                    }
+                    __syncthreads();
+                    if (active) {
+                        int nk = min(C::FKB, NFK - fk0);
+                        for (int o = lane; o < nk * NFL; o += TPQ) {
+                            double s = 0;
+                            for (int t = 0; t < C::NIJ; t++) s += Sj[o * C::NIJ + t];
+                            int fk = fk0 + o / NFL, fl = o % NFL;
+                            atomicAdd(VJ + (size_t)(Q.k0 + fk) * nao + Q.l0 + fl, s);
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// dispatch
+
+static inline int task_tiles(const JKTask &task) {
+    return ((task.na + TILE - 1) / TILE) * ((task.nb + TILE - 1) / TILE);
+}
+
+template <int LI, int LJ, int LK, int LL>
+static int launch_small(const JKArgs &args, const JKTask &task, int fp32, cudaStream_t stream) {
+    int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
+    if (ntiles == 0) return 0;
+    if (fp32)
+        jk_small<LI, LJ, LK, LL, float><<<ntiles, 256, 0, stream>>>(args, task);
+    else
+        jk_small<LI, LJ, LK, LL, double><<<ntiles, 256, 0, stream>>>(args, task);
+    return 0;
+}
+
+template <int LI, int LJ, int LK, int LL, int NSPLIT>
+static int launch_group(const JKArgs &args, const JKTask &task, cudaStream_t stream) {
+    using C = GroupCfg<LI, LJ, LK, LL, NSPLIT>;
+    static_assert(C::SMEM + 2048 <= 227 * 1024, "shared memory per CTA");
+    static_assert(C::NT <= 1024, "threads per CTA");
+    int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
+    if (ntiles == 0) return 0;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(jk_group<LI, LJ, LK, LL, NSPLIT>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+        configured = true;
+    }
+    jk_group<LI, LJ, LK, LL, NSPLIT><<<ntiles, C::NT, C::SMEM, stream>>>(args, task);
+    return 0;
+}
+
+// Bra side = pair (LI, LJ) (threads), ket side = pair (LK, LL) (accumulators).
+// Small classes run one thread per quartet; larger ones put the pair with
+// fewer Cartesian components on the thread side and split the ket
+// components into chunks of at most ~36 accumulators.
+template <int L1, int L2, int L3, int L4>
+static int launch_class(const JKArgs &args, const JKTask &task, int fp32, cudaStream_t stream) {
+    constexpr int N12 = ncart(L1) * ncart(L2), N34 = ncart(L3) * ncart(L4);
+    if constexpr (N12 * N34 <= SMALL_NF) {
+        return launch_small<L1, L2, L3, L4>(args, task, fp32, stream);
+    } else if constexpr (N12 <= N34) {
+        constexpr int NS = cdiv(N34, 36) > ncart(L3) ? ncart(L3) : cdiv(N34, 36);
+        return launch_group<L1, L2, L3, L4, NS>(args, task, stream);
+    } else {
+        constexpr int NS = cdiv(N12, 36) > ncart(L1) ? ncart(L1) : cdiv(N12, 36);
+        JKTask sw = task;
+        sw.a0 = task.b0; sw.na = task.nb; sw.b0 = task.a0; sw.nb = task.na;
+        sw.pa0 = task.pb0; sw.pb0 = task.pa0; sw.nprim_a = task.nprim_b; sw.nprim_b = task.nprim_a;
+        sw.rows_are_b = !task.rows_are_b;
+        // diag tasks have identical lists on both sides; the a >= b rule stays
+        return launch_group<L3, L4, L1, L2, NS>(args, sw, stream);
+    }
+}
+
+}  // namespace bqc

@@ -1,0 +1,130 @@
+/*
+ * C ABI of libbyteqc_b200.so, the B200 (sm_100a) direct-SCF J/K engine.
+ *
+ * Two levels of entry points:
+ *
+ * 1. Drop-in replacements for the reference's libgint/libgvhf symbols that
+ *    cuobc/scf/hf.py binds through ctypes.  Names, argument order, argument
+ *    meaning, struct layouts and return codes are the reference's, so hf.py
+ *    can load this library in place of libgint.so and libgvhf.so.
+ *
+ * 2. Native whole-build entry points (BQC*), used by this package's own
+ *    get_jk: one call screens every quartet on the device against
+ *    q_ij q_kl max|D| and builds J and K for all class pairs, replacing the
+ *    host loop over class pairs and bins (cuobc/scf/hf.py:111-166).
+ *
+ * Conventions shared by both levels: Cartesian AOs of the sorted,
+ * decontracted basis; dm, vj, vk are n_dm x nao x nao FP64 device arrays;
+ * vj/vk are accumulated (the caller zeroes them) with the per-quartet
+ * contributions V, and the caller forms J = 2 (V + V^T), K = V + V^T
+ * (cuobc/scf/hf.py:171-181).  A NULL vj or vk disables that output.
+ * Return codes: 0 ok, 1 CUDA error or unsupported class, 2 angular momentum
+ * beyond f (the reference returns 2 for nroots >= 12).
+ */
+#ifndef BYTEQC_B200_H
+#define BYTEQC_B200_H
+
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same layout as the reference's ContractionProdType
+ * (cuobc/lib/gint/gint.h:101-107). */
+typedef struct {
+    int l_bra;
+    int l_ket;
+    int nprim_12;
+    int npairs;
+} ContractionProdType;
+
+/* Same layout as the reference's BasisProdCache (cuobc/lib/gint/gint.h:118-147);
+ * hf.py reads aexyz and primitive_pairs_locs through ctypes. */
+typedef struct {
+    int nbas;
+    int ncptype;
+    ContractionProdType *cptype;
+    int *bas_pairs_locs;
+    int *primitive_pairs_locs;
+    int *bas_pair2shls;
+    double *aexyz;
+
+    double *bas_coords;
+    int *bas_pair2bra;
+    int *bas_pair2ket;
+    int *ao_loc;
+    double *a12;
+    double *e12;
+    double *x12;
+    double *y12;
+    double *z12;
+} BasisProdCache;
+
+/* ---- level 1: the reference's entry points -------------------------------- */
+
+/* Replaces GINTinit_basis_prod_cpu (cuobc/lib/gint/nr_fill_ao_ints.cu:452-470):
+ * builds the class table and the host primitive-pair block
+ * aexyz = [a12 | e12 | x12 | y12 | z12] and fills bas_coords (3 x nbas, host). */
+void GINTinit_basis_prod_cpu(BasisProdCache **pbp, double diag_fac, double *bas_coords,
+                             int *bas_pair2shls, int *bas_pairs_locs, int ncptype,
+                             int *atm, int natm, int *bas, int nbas, double *env);
+
+/* Replaces GINTinit_basis_prod_gpu (cuobc/lib/gint/nr_fill_ao_ints.cu:472-491):
+ * copies the host cache and points it at device copies of ao_loc, bas_coords,
+ * aexyz and bas_pair2shls (device pointers owned by the caller). */
+void GINTinit_basis_prod_gpu(BasisProdCache **pbpin, BasisProdCache **pbp, int *ao_loc,
+                             double *bas_coords, double *aexyz, int *bas_pair2shls);
+
+/* Replaces GINTdel_basis_prod (cuobc/lib/gint/nr_fill_ao_ints.cu:394-410). */
+void GINTdel_basis_prod(BasisProdCache **pbp);
+
+/* Replaces GINTbuild_jk (cuobc/lib/gvhf/nr_jk_driver.cu:227-284): J/K
+ * contributions of class pair (cp_ij_id, cp_kl_id) over the binned pair
+ * ranges, kl bin b paired with ij bins [0, nbins - b). */
+int GINTbuild_jk(BasisProdCache *bpcache, double *vj, double *vk, double *dm, int nao,
+                 int n_dm, int *bins_locs_ij, int *bins_locs_kl, int nbins, int cp_ij_id,
+                 int cp_kl_id, cudaStream_t stream);
+
+/* ---- level 2: native whole-build entry points ------------------------------ */
+
+/* All class pairs of one J/K build (no reference counterpart; it replaces the
+ * per-class-pair loop of cuobc/scf/hf.py:111-166).  pair_q: device Schwarz
+ * factor of every pair (same order as bas_pair2shls, sorted descending within
+ * each class); pair_q_host: the same on the host, used to launch only the
+ * 16 x 16 quartet tiles whose largest bound q_ij q_kl dm_max reaches tol
+ * (NULL launches every tile); dm_cond: device nbas x nbas block max |D| (see
+ * BQCdm_cond), NULL screens on Schwarz alone; dm_max: max of dm_cond.
+ * tol: the direct-SCF threshold.  fp32_below: quartets whose bound
+ * q_ij q_kl max|D| is below it are evaluated in FP32 (0 keeps all FP64).
+ * status_dev: optional device int set nonzero on an internal error. */
+int BQCbuild_jk(const BasisProdCache *bpcache, const double *pair_q, const double *pair_q_host,
+                const double *dm_cond, double dm_max, double *vj, double *vk, const double *dm,
+                int nao, int n_dm, double tol, double fp32_below, int *status_dev,
+                cudaStream_t stream);
+
+/* Block max |D| per shell pair: dm_cond[i * nbas + j] = max over n_dm and the
+ * AOs of shells i, j of |dm|.  ao_loc is a device array (nbas + 1). */
+int BQCdm_cond(const double *dm, int n_dm, int nao, const int *ao_loc, int nbas,
+               double *dm_cond, cudaStream_t stream);
+
+/* Schwarz factors sqrt(max |(ij|ij)|) of the pairs [p0, p0 + np) of class cp,
+ * computed on the device (the reference takes them from libcint on the CPU,
+ * cuobc/scf/hf.py:341).  The e12 diagonal factor is undone. */
+int BQCschwarz(const BasisProdCache *bpcache, int cp, double diag_fac, double *q_out,
+               cudaStream_t stream);
+
+/* One-electron integrals over the Cartesian AOs of shells given in pyscf
+ * layout (device copies of atm, bas, env, ao_loc): overlap, kinetic and
+ * nuclear attraction, each nao x nao (any may be NULL). */
+int BQCint1e(const int *atm, int natm, const int *bas, int nbas, const double *env,
+             const int *ao_loc, int nao, double *S, double *T, double *V,
+             cudaStream_t stream);
+
+/* Library version string. */
+const char *BQCversion(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
