@@ -44,12 +44,17 @@ struct JKTask {
     int rows_are_b;
 };
 
+// number of kernel launches issued by the library so far (all threads)
+unsigned long long bqc_count_launch(int n);
+
 // device address of the Rys coefficient table on the current device (rys_table.cu)
 const double *bqc_rys_table();
 
 // launchers (jk_dispatch.cu, schwarz.cu)
 int bqc_launch_jk(int li, int lj, int lk, int ll, const JKArgs &args, const JKTask &task,
                   int fp32, cudaStream_t stream);
+int bqc_launch_count(const JKArgs &args, const JKTask &task, unsigned long long *count,
+                     cudaStream_t stream);
 int bqc_launch_dm_cond(const double *dm, int n_dm, int nao, const int *ao_loc, int nbas,
                        double *dm_cond, cudaStream_t stream);
 int bqc_launch_schwarz(int li, int lj, const JKArgs &args, int p0, int np, int pa0, int nprim,

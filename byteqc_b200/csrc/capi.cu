@@ -207,11 +207,13 @@ static int tile_rows(const double *qa, int na, const double *qb, int nb, double 
     return prefix.back() - prefix[base];
 }
 
-int BQCbuild_jk(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
-                const double *dm_cond, double dm_max, double *vj, double *vk, const double *dm,
-                int nao, int n_dm, double tol, double fp32_below, int *status_dev,
-                cudaStream_t stream) {
-    (void)fp32_below;
+// Launch (or, with count_dev, only count the surviving quartets of) every
+// class pair, or the single class pair (only_ij, only_kl) when only_ij >= 0.
+static int build_jk_impl(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
+                         const double *dm_cond, double dm_max, double *vj, double *vk,
+                         const double *dm, int nao, int n_dm, double tol, double fp32_below,
+                         int *status_dev, int only_ij, int only_kl,
+                         unsigned long long *count_dev, cudaStream_t stream) {
     JKArgs args = make_args(bp, vj, vk, dm, nao, n_dm);
     args.pair_q = pair_q;
     args.dm_cond = dm_cond;
@@ -225,9 +227,11 @@ int BQCbuild_jk(const BasisProdCache *bp, const double *pair_q, const double *pa
     for (int cij = 0; cij < bp->ncptype; cij++) {
         const ContractionProdType *tij = bp->cptype + cij;
         if (tij->npairs == 0) continue;
+        if (only_ij >= 0 && cij != only_ij) continue;
         for (int ckl = 0; ckl <= cij; ckl++) {
             const ContractionProdType *tkl = bp->cptype + ckl;
             if (tkl->npairs == 0) continue;
+            if (only_kl >= 0 && ckl != only_kl) continue;
             if (tij->l_bra > BQC_LMAX || tkl->l_bra > BQC_LMAX) return 2;
             JKTask t;
             memset(&t, 0, sizeof(t));
@@ -270,11 +274,40 @@ int BQCbuild_jk(const BasisProdCache *bp, const double *pair_q, const double *pa
     int err = 0;
     for (size_t i = 0; i < tasks.size() && !err; i++) {
         if (d_prefix) tasks[i].tile_prefix = d_prefix + prefix_off[i];
-        err = bqc_launch_jk(shape[4 * i], shape[4 * i + 1], shape[4 * i + 2], shape[4 * i + 3],
-                            args, tasks[i], 0, stream);
+        if (count_dev != nullptr)
+            err = bqc_launch_count(args, tasks[i], count_dev, stream);
+        else
+            err = bqc_launch_jk(shape[4 * i], shape[4 * i + 1], shape[4 * i + 2], shape[4 * i + 3],
+                                args, tasks[i], 0, stream);
     }
     if (d_prefix) cudaFreeAsync(d_prefix, stream);
+    (void)fp32_below;
     return err;
+}
+
+int BQCbuild_jk(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
+                const double *dm_cond, double dm_max, double *vj, double *vk, const double *dm,
+                int nao, int n_dm, double tol, double fp32_below, int *status_dev,
+                cudaStream_t stream) {
+    return build_jk_impl(bp, pair_q, pair_q_host, dm_cond, dm_max, vj, vk, dm, nao, n_dm, tol,
+                         fp32_below, status_dev, -1, -1, nullptr, stream);
+}
+
+int BQCbuild_jk_class(const BasisProdCache *bp, int cp_ij, int cp_kl, const double *pair_q,
+                      const double *pair_q_host, const double *dm_cond, double dm_max, double *vj,
+                      double *vk, const double *dm, int nao, int n_dm, double tol,
+                      double fp32_below, int *status_dev, cudaStream_t stream) {
+    if (cp_ij < 0 || cp_kl < 0 || cp_kl > cp_ij || cp_ij >= bp->ncptype) return 1;
+    return build_jk_impl(bp, pair_q, pair_q_host, dm_cond, dm_max, vj, vk, dm, nao, n_dm, tol,
+                         fp32_below, status_dev, cp_ij, cp_kl, nullptr, stream);
+}
+
+int BQCcount_quartets(const BasisProdCache *bp, int cp_ij, int cp_kl, const double *pair_q,
+                      const double *pair_q_host, const double *dm_cond, double dm_max, double tol,
+                      unsigned long long *count_dev, cudaStream_t stream) {
+    if (count_dev == nullptr) return 1;
+    return build_jk_impl(bp, pair_q, pair_q_host, dm_cond, dm_max, nullptr, nullptr, nullptr, 0, 0,
+                         tol, 0., nullptr, cp_ij, cp_kl, count_dev, stream);
 }
 
 int BQCdm_cond(const double *dm, int n_dm, int nao, const int *ao_loc, int nbas, double *dm_cond,

@@ -208,6 +208,7 @@ extern "C" int BQCint1e(const int *atm, int natm, const int *bas, int nbas, cons
         auto &l = lists[key];
         if (l.empty()) continue;
         cudaMemcpyAsync(dpairs + off, l.data(), sizeof(int) * l.size(), cudaMemcpyHostToDevice, stream);
+        bqc_count_launch(1);
         int np = (int)l.size() / 2;
         int nb = (np * ((key / 4 + 1) * (key / 4 + 2) / 2) + 127) / 128;
         switch (key) {

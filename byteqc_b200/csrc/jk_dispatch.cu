@@ -4,7 +4,7 @@
 // compile in parallel.
 #include <stdio.h>
 #include <utility>
-#include "bqc.h"
+#include "jk_kernels.cuh"
 
 #define BQC_CASE(a, b, c, d) \
     int bqc_class_##a##b##c##d(const JKArgs &, const JKTask &, int, cudaStream_t);
@@ -13,8 +13,15 @@
 
 
 // (li, lj | lk, ll) with li >= lj, lk >= ll, l <= 3.
+static unsigned long long g_launches = 0;
+
+unsigned long long bqc_count_launch(int n) { return __atomic_add_fetch(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+
+extern "C" unsigned long long BQClaunch_counter(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+
 int bqc_launch_jk(int li, int lj, int lk, int ll, const JKArgs &args, const JKTask &task,
                   int fp32, cudaStream_t stream) {
+    bqc_count_launch(1);
     if (li < lj || lk < ll || li > BQC_LMAX || lk > BQC_LMAX) return 2;
     // canonical order: pair index (l1*(l1+1)/2 + l2) of the bra >= that of the ket
     int pij = li * (li + 1) / 2 + lj, pkl = lk * (lk + 1) / 2 + ll;
@@ -75,7 +82,28 @@ int bqc_launch_dm_cond(const double *dm, int n_dm, int nao, const int *ao_loc, i
                        double *dm_cond, cudaStream_t stream) {
     dim3 block(8, 32);
     dim3 grid((nbas + 31) / 32, nbas);
+    bqc_count_launch(1);
     dm_cond_kernel<<<grid, block, 0, stream>>>(dm, n_dm, nao, ao_loc, nbas, dm_cond);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }
 
+
+// ---------------------------------------------------------------------------
+// surviving-quartet count of one task (same tiles and screening as the J/K
+// kernels, no integrals): the denominator of the algorithmic FLOP count
+__global__ void count_kernel(JKArgs A, JKTask T, unsigned long long *count) {
+    __shared__ int s_list[bqc::TILE * bqc::TILE];
+    __shared__ int s_count;
+    int a_begin, b_begin, n;
+    if (!bqc::tile_screen(A, T, s_list, &s_count, a_begin, b_begin, n)) return;
+    if (threadIdx.x == 0) atomicAdd(count, (unsigned long long)n);
+}
+
+int bqc_launch_count(const JKArgs &args, const JKTask &task, unsigned long long *count,
+                     cudaStream_t stream) {
+    int ntiles = task.tile_prefix ? task.ntiles : bqc::task_tiles(task);
+    if (ntiles == 0) return 0;
+    bqc_count_launch(1);
+    count_kernel<<<ntiles, 256, 0, stream>>>(args, task, count);
+    return cudaGetLastError() == cudaSuccess ? 0 : 1;
+}

@@ -72,6 +72,7 @@ int bqc_launch_schwarz(int li, int lj, const JKArgs &args, int p0, int np, int p
                        double diag_fac, double *q_out, cudaStream_t stream) {
     if (np <= 0) return 0;
     int nb = (np + 127) / 128;
+    bqc_count_launch(1);
     switch (li * 4 + lj) {
 #define BQC_SCASE(a, b)                                                                        \
     case a * 4 + b:                                                                            \

@@ -15,7 +15,8 @@ _lib = None
 
 # exported symbols, as declared in include/byteqc_b200.h
 SYMBOLS = ('GINTinit_basis_prod_cpu', 'GINTinit_basis_prod_gpu', 'GINTdel_basis_prod',
-           'GINTbuild_jk', 'BQCbuild_jk', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e',
+           'GINTbuild_jk', 'BQCbuild_jk', 'BQCbuild_jk_class', 'BQCcount_quartets',
+           'BQCfp64_fma_peak', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e', 'BQClaunch_counter',
            'BQCversion')
 
 
@@ -29,12 +30,20 @@ def load_library(name='libbyteqc_b200'):
                            '(the J/K engine has no CPU fallback)' % LIBPATH)
     lib = ctypes.CDLL(LIBPATH)
     lib.BQCversion.restype = ctypes.c_char_p
+    lib.BQClaunch_counter.restype = ctypes.c_ulonglong
     for fn in ('GINTbuild_jk', 'BQCbuild_jk', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e'):
         getattr(lib, fn).restype = ctypes.c_int
     # double arguments must be declared where a bare Python float is passed
     lib.BQCbuild_jk.argtypes = [ctypes.c_void_p] * 4 + [ctypes.c_double] + [ctypes.c_void_p] * 3 + \
         [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
          ctypes.c_void_p]
+    lib.BQCbuild_jk_class.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + \
+        [ctypes.c_void_p] * 3 + [ctypes.c_double] + [ctypes.c_void_p] * 3 + \
+        [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+         ctypes.c_void_p]
+    lib.BQCcount_quartets.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + \
+        [ctypes.c_void_p] * 3 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                 ctypes.c_void_p]
     lib.GINTinit_basis_prod_cpu.restype = None
     lib.GINTinit_basis_prod_gpu.restype = None
     lib.GINTdel_basis_prod.restype = None

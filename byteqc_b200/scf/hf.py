@@ -477,6 +477,7 @@ class RHF(_SCFBase):
     """
 
     rebuild_cycle = 8
+    jk_hook = None   # optional callable(density) run after each J/K build (accounting)
 
     def init_guess_dm(self):
         from .guess import init_guess
@@ -511,13 +512,17 @@ class RHF(_SCFBase):
         for cycle in range(self.max_cycle):
             tj = time.perf_counter()
             if dm_last is None or cycle % self.rebuild_cycle == 0:
+                dm_in = dm
                 vj, vk = opt.jk_ao(dm[None])
             else:
-                dvj, dvk = opt.jk_ao((dm - dm_last)[None])
+                dm_in = dm - dm_last
+                dvj, dvk = opt.jk_ao(dm_in[None])
                 vj = vj + dvj
                 vk = vk + dvk
             torch.cuda.synchronize()
             t_jk += time.perf_counter() - tj
+            if self.jk_hook is not None:
+                self.jk_hook(dm_in)
             F = h + vj[0] - .5 * vk[0]
             e = float(.5 * torch.sum(dm * (h + F))) + e_nuc
             self.cycles = cycle + 1
@@ -541,6 +546,68 @@ class RHF(_SCFBase):
         return self.e_tot
 
     scf = kernel
+
+    def kernel_hostloop(self, dm0=None):
+        """The reference's arrangement of one SCF: a CPU loop (pyscf's role)
+        holding host numpy arrays, calling the drop-in ``get_jk`` with a host
+        density every cycle (host->device copy of D, device->host copies of J
+        and K) and ``_eigh`` with host matrices (cuobc/scf/hf.py:230-274).
+        Returns the energy; ``self.host_bytes`` = (h2d, d2h) bytes moved by
+        get_jk and _eigh."""
+        t0 = time.perf_counter()
+        S = self.get_ovlp().cpu().numpy()
+        h = self.get_hcore().cpu().numpy()
+        e_nuc = self.energy_nuc()
+        dm = (self.init_guess_dm() if dm0 is None else torch.as_tensor(dm0)).cpu().numpy()
+        nao = dm.shape[0]
+        nocc = self.mol.nelectron // 2
+        h2d = d2h = 0
+        focks, errs = [], []
+        e_last = None
+        vj = vk = dm_last = None
+        self.converged = False
+        for cycle in range(self.max_cycle):
+            if dm_last is None or cycle % self.rebuild_cycle == 0:
+                vj, vk = self.get_jk(self.mol, dm)
+            else:
+                dvj, dvk = self.get_jk(self.mol, dm - dm_last)
+                vj, vk = vj + dvj, vk + dvk
+            h2d += dm.nbytes
+            d2h += 2 * dm.nbytes
+            F = h + vj - .5 * vk
+            e = float(.5 * np.sum(dm * (h + F))) + e_nuc
+            self.cycles = cycle + 1
+            if e_last is not None and abs(e - e_last) < self.conv_tol:
+                self.converged = True
+                break
+            e_last = e
+            focks.append(F)
+            errs.append((F @ dm @ S - S @ dm @ F).ravel())
+            focks, errs = focks[-self.diis_space:], errs[-self.diis_space:]
+            n = len(focks)
+            if n > 1:
+                B = -np.ones((n + 1, n + 1))
+                B[n, n] = 0
+                E = np.array(errs)
+                B[:n, :n] = E @ E.T
+                rhs = np.zeros(n + 1)
+                rhs[n] = -1
+                c = np.linalg.solve(B, rhs)[:n]
+                Fd = np.einsum('i,ijk->jk', c, np.array(focks))
+            else:
+                Fd = F
+            mo_e, mo_c = self._eigh(Fd, S)
+            mo_e = mo_e.cpu().numpy()
+            mo_c = mo_c.cpu().numpy()
+            h2d += Fd.nbytes + S.nbytes
+            d2h += mo_e.nbytes + mo_c.nbytes
+            idx = np.argsort(mo_e)[:nocc]
+            dm_last = dm
+            dm = 2. * mo_c[:, idx] @ mo_c[:, idx].T
+        self.e_tot = e
+        self.host_bytes = (h2d, d2h)
+        self.timings['total'] = time.perf_counter() - t0
+        return e
 
 
 class UHF(_SCFBase):

@@ -103,6 +103,25 @@ int BQCbuild_jk(const BasisProdCache *bpcache, const double *pair_q, const doubl
                 int nao, int n_dm, double tol, double fp32_below, int *status_dev,
                 cudaStream_t stream);
 
+/* One class pair (cp_ij >= cp_kl) of BQCbuild_jk, same arguments otherwise;
+ * lets a caller time or profile the kernels class by class. */
+int BQCbuild_jk_class(const BasisProdCache *bpcache, int cp_ij, int cp_kl, const double *pair_q,
+                      const double *pair_q_host, const double *dm_cond, double dm_max,
+                      double *vj, double *vk, const double *dm, int nao, int n_dm, double tol,
+                      double fp32_below, int *status_dev, cudaStream_t stream);
+
+/* Number of quartets of class pair (cp_ij, cp_kl) (all class pairs when
+ * cp_ij < 0) that pass the screening of BQCbuild_jk, added to the device
+ * counter *count_dev; no integrals are evaluated. */
+int BQCcount_quartets(const BasisProdCache *bpcache, int cp_ij, int cp_kl, const double *pair_q,
+                      const double *pair_q_host, const double *dm_cond, double dm_max,
+                      double tol, unsigned long long *count_dev, cudaStream_t stream);
+
+/* FP64 FMA throughput of the current device in FLOP/s, measured by a
+ * dependent-chain DFMA microbenchmark (the roofline denominator of the J/K
+ * kernels); ms_out (may be NULL) receives the timed kernel's duration. */
+int BQCfp64_fma_peak(double *flops_per_s, float *ms_out);
+
 /* Block max |D| per shell pair: dm_cond[i * nbas + j] = max over n_dm and the
  * AOs of shells i, j of |dm|.  ao_loc is a device array (nbas + 1). */
 int BQCdm_cond(const double *dm, int n_dm, int nao, const int *ao_loc, int nbas,
@@ -120,6 +139,9 @@ int BQCschwarz(const BasisProdCache *bpcache, int cp, double diag_fac, double *q
 int BQCint1e(const int *atm, int natm, const int *bas, int nbas, const double *env,
              const int *ao_loc, int nao, double *S, double *T, double *V,
              cudaStream_t stream);
+
+/* Number of kernel launches the library has issued in this process. */
+unsigned long long BQClaunch_counter(void);
 
 /* Library version string. */
 const char *BQCversion(void);
