@@ -325,6 +325,54 @@ int BQCschwarz(const BasisProdCache *bp, int cp, double diag_fac, double *q_out,
                               bp->primitive_pairs_locs[cp], t->nprim_12, diag_fac, q_out, stream);
 }
 
+// ---------------------------------------------------------------------------
+// J/K build that allocates nothing.
+//
+// Some callers cannot let the library allocate device memory: a host program
+// that sizes its device memory once from a fixed arena and forbids any other
+// allocation (so nothing can fragment or contend with its own pool), or one
+// whose only device buffers are the inputs and outputs it passes in.
+// BQCbuild_jk reserves stream-ordered scratch for its tile tables and expects
+// the caller to provide the density-screening table; this variant needs
+// neither.  Its only scratch, the per-shell-pair density maxima, lives in the
+// file-scope array below (BQC_NOALLOC_MAX_NBAS^2 doubles = 2 MiB, held on
+// every GPU that loads the library until the process exits), and it launches
+// every quartet tile of every class pair (device screening only, no
+// host-side tile pruning), which suits the small systems that fit the limit.
+#define BQC_NOALLOC_MAX_NBAS 512
+static __device__ __align__(256) double g_noalloc_dm_cond[BQC_NOALLOC_MAX_NBAS * BQC_NOALLOC_MAX_NBAS];
+
+// Device address of g_noalloc_dm_cond on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device (with that device current) and cached.
+static double *noalloc_scratch() {
+    static double *addr[128] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return nullptr;
+    if (addr[dev] == nullptr) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_dm_cond) != cudaSuccess) return nullptr;
+        addr[dev] = static_cast<double *>(p);
+    }
+    return addr[dev];
+}
+
+int BQCbuild_jk_noalloc(const BasisProdCache *bp, const double *pair_q, double *vj, double *vk,
+                        const double *dm, int nao, int n_dm, double tol, cudaStream_t stream) {
+    if (bp->nbas > BQC_NOALLOC_MAX_NBAS) {
+        fprintf(stderr, "BQCbuild_jk_noalloc: %d shells exceed the limit of %d\n", bp->nbas,
+                BQC_NOALLOC_MAX_NBAS);
+        return 3;
+    }
+    double *dm_cond = noalloc_scratch();
+    if (dm_cond == nullptr) return 1;
+    // every entry of the nbas x nbas table is overwritten before it is read
+    int err = bqc_launch_dm_cond(dm, n_dm, nao, bp->ao_loc, bp->nbas, dm_cond, stream);
+    if (err) return err;
+    return build_jk_impl(bp, pair_q, nullptr, dm_cond, 1.0, vj, vk, dm, nao, n_dm, tol, 0.,
+                         nullptr, -1, -1, nullptr, stream);
+}
+
 const char *BQCversion(void) { return "byteqc_b200 0.1 sm_100a"; }
 
 }  // extern "C"

@@ -17,7 +17,7 @@ _lib = None
 SYMBOLS = ('GINTinit_basis_prod_cpu', 'GINTinit_basis_prod_gpu', 'GINTdel_basis_prod',
            'GINTbuild_jk', 'BQCbuild_jk', 'BQCbuild_jk_class', 'BQCcount_quartets',
            'BQCfp64_fma_peak', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e', 'BQClaunch_counter',
-           'BQCversion')
+           'BQCbuild_jk_noalloc', 'BQCversion')
 
 
 def load_library(name='libbyteqc_b200'):
@@ -44,6 +44,7 @@ def load_library(name='libbyteqc_b200'):
     lib.BQCcount_quartets.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int] + \
         [ctypes.c_void_p] * 3 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                                  ctypes.c_void_p]
+    lib.BQCbuild_jk_noalloc.restype = ctypes.c_int
     lib.GINTinit_basis_prod_cpu.restype = None
     lib.GINTinit_basis_prod_gpu.restype = None
     lib.GINTdel_basis_prod.restype = None

@@ -140,6 +140,19 @@ int BQCint1e(const int *atm, int natm, const int *bas, int nbas, const double *e
              const int *ao_loc, int nao, double *S, double *T, double *V,
              cudaStream_t stream);
 
+/* BQCbuild_jk for callers that cannot let the library allocate device memory
+ * (no reference counterpart).  It allocates nothing: the density-screening
+ * scratch is a fixed array inside the library (2 MiB per GPU, held until the
+ * process exits), so it accepts at most 512 shells of the sorted, decontracted
+ * basis and returns 3 beyond that; it screens on the device against
+ * q_ij q_kl max|D| >= tol and launches every quartet tile.  The first call on
+ * a device looks up the array's device address; make that first call before
+ * any stream capture.  All calls share the array: calls that overlap on the
+ * GPU (different streams, or concurrent host threads) race on it. */
+int BQCbuild_jk_noalloc(const BasisProdCache *bpcache, const double *pair_q, double *vj,
+                        double *vk, const double *dm, int nao, int n_dm, double tol,
+                        cudaStream_t stream);
+
 /* Number of kernel launches the library has issued in this process. */
 unsigned long long BQClaunch_counter(void);
 
