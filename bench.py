@@ -226,7 +226,7 @@ def scf_flops(mol, conv):
     mf = hf.RHF(mol)
     mf.conv_tol = conv
     acc = []
-    mf.jk_hook = lambda d: acc.append(jk_flops(mf.opt, d))
+    mf.jk_hook = lambda d, fp32_below: acc.append(jk_flops(mf.opt, d))
     mf.kernel()
     return float(sum(acc)), len(acc)
 

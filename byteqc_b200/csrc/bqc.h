@@ -20,6 +20,7 @@ struct JKArgs {
     double *vj, *vk;          // [n_dm][nao][nao] accumulated (NULL disables)
     int nao, nbas, n_dm;
     double tol;               // drop quartets with q_ij q_kl max|D| < tol
+    double tol_hi;            // and, when > 0, those with a bound >= tol_hi (FP32 band)
     int *status;              // device error word (0 = ok), may be NULL
     const double *rys;        // Rys coefficient table (bqc_rys_table())
 };

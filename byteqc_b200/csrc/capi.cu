@@ -132,6 +132,7 @@ static JKArgs make_args(const BasisProdCache *bp, double *vj, double *vk, const 
                         int nao, int n_dm) {
     JKArgs a;
     memset(&a, 0, sizeof(a));
+    a.tol_hi = 0.;
     a.pair_bra = bp->bas_pair2bra;
     a.pair_ket = bp->bas_pair2ket;
     a.a12 = bp->a12;
@@ -209,17 +210,9 @@ static int tile_rows(const double *qa, int na, const double *qb, int nb, double 
 
 // Launch (or, with count_dev, only count the surviving quartets of) every
 // class pair, or the single class pair (only_ij, only_kl) when only_ij >= 0.
-static int build_jk_impl(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
-                         const double *dm_cond, double dm_max, double *vj, double *vk,
-                         const double *dm, int nao, int n_dm, double tol, double fp32_below,
-                         int *status_dev, int only_ij, int only_kl,
+static int build_jk_band(const BasisProdCache *bp, JKArgs args, const double *pair_q_host,
+                         double dm_max, int fp32, int only_ij, int only_kl,
                          unsigned long long *count_dev, cudaStream_t stream) {
-    JKArgs args = make_args(bp, vj, vk, dm, nao, n_dm);
-    args.pair_q = pair_q;
-    args.dm_cond = dm_cond;
-    args.tol = tol;
-    args.status = status_dev;
-    if (dm_cond == nullptr) dm_max = 1.0;
     std::vector<JKTask> tasks;
     std::vector<int> shape;   // (li, lj, lk, ll) per task
     std::vector<int> prefix;
@@ -247,8 +240,8 @@ static int build_jk_impl(const BasisProdCache *bp, const double *pair_q, const d
             t.skip_lower = 1;
             if (pair_q_host != nullptr) {
                 size_t off = prefix.size();
-                int n = tile_rows(pair_q_host + t.a0, t.na, pair_q_host + t.b0, t.nb, dm_max, tol,
-                                  t.diag, prefix);
+                int n = tile_rows(pair_q_host + t.a0, t.na, pair_q_host + t.b0, t.nb, dm_max,
+                                  args.tol, t.diag, prefix);
                 if (n == 0) {
                     prefix.resize(off);
                     continue;
@@ -278,11 +271,37 @@ static int build_jk_impl(const BasisProdCache *bp, const double *pair_q, const d
             err = bqc_launch_count(args, tasks[i], count_dev, stream);
         else
             err = bqc_launch_jk(shape[4 * i], shape[4 * i + 1], shape[4 * i + 2], shape[4 * i + 3],
-                                args, tasks[i], 0, stream);
+                                args, tasks[i], fp32, stream);
     }
     if (d_prefix) cudaFreeAsync(d_prefix, stream);
-    (void)fp32_below;
     return err;
+}
+
+// Launch (or, with count_dev, only count the surviving quartets of) every
+// class pair, or the single class pair (only_ij, only_kl) when only_ij >= 0.
+// With fp32_below > tol the quartets split into two bands: bound >= fp32_below
+// in FP64 and tol <= bound < fp32_below in FP32 (count_dev counts both).
+static int build_jk_impl(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
+                         const double *dm_cond, double dm_max, double *vj, double *vk,
+                         const double *dm, int nao, int n_dm, double tol, double fp32_below,
+                         int *status_dev, int only_ij, int only_kl,
+                         unsigned long long *count_dev, cudaStream_t stream) {
+    JKArgs args = make_args(bp, vj, vk, dm, nao, n_dm);
+    args.pair_q = pair_q;
+    args.dm_cond = dm_cond;
+    args.tol = tol;
+    args.tol_hi = 0.;
+    args.status = status_dev;
+    if (dm_cond == nullptr) dm_max = 1.0;
+    if (pair_q == nullptr || fp32_below <= tol)
+        return build_jk_band(bp, args, pair_q_host, dm_max, 0, only_ij, only_kl, count_dev, stream);
+    JKArgs hi = args;
+    hi.tol = fp32_below;
+    int err = build_jk_band(bp, hi, pair_q_host, dm_max, 0, only_ij, only_kl, count_dev, stream);
+    if (err) return err;
+    JKArgs lo = args;
+    lo.tol_hi = fp32_below;
+    return build_jk_band(bp, lo, pair_q_host, dm_max, 1, only_ij, only_kl, count_dev, stream);
 }
 
 int BQCbuild_jk(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,

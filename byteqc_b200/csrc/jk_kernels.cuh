@@ -28,7 +28,7 @@
 namespace bqc {
 
 constexpr int TILE = 16;
-constexpr int SMALL_NF = 36;
+constexpr int SMALL_NF = 54;
 constexpr double TWO_PI_2P5 = 34.986836655249725693;  // 2 pi^(5/2)
 
 // ---------------------------------------------------------------------------
@@ -79,7 +79,7 @@ __device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, in
                 int k = __ldg(A.pair_bra + b), l = __ldg(A.pair_ket + b);
                 bound *= dmax6(A.dm_cond, A.nbas, i, j, k, l);
             }
-            keep = bound >= A.tol;
+            keep = bound >= A.tol && (A.tol_hi <= 0. || bound < A.tol_hi);
         }
         if (keep) {
             int idx = atomicAdd(s_count, 1);
@@ -314,6 +314,338 @@ __global__ void __launch_bounds__(256) jk_small(JKArgs A, JKTask T) {
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// fixed-layout tile kernel: thread (row, col) of a 256-thread CTA evaluates
+// quartet (bra pair a_begin + row, ket pair b_begin + col) in registers.
+// Contributions that share a target are summed across the tile before the
+// atomics: J_ij over the 16 kets of a row, J_kl over the 16 bras of a
+// column (warp shuffles, then shared memory across the 8 warps); when all
+// bra pairs of the tile share the bra shell i (the pair lists are laid out
+// that way, see _tile_order) K_il is summed over a column, when all ket
+// pairs share k, K_jk over a row, and K_ik over both.
+template <int NV>
+__device__ __forceinline__ void row_reduce(double (&v)[NV]) {
+#pragma unroll
+    for (int n = 0; n < NV; n++) {
+        double x = v[n];
+        x += __shfl_xor_sync(0xffffffffu, x, 8);
+        x += __shfl_xor_sync(0xffffffffu, x, 4);
+        x += __shfl_xor_sync(0xffffffffu, x, 2);
+        x += __shfl_xor_sync(0xffffffffu, x, 1);
+        v[n] = x;
+    }
+}
+
+// Sum v over the 16 rows of the tile for each column; afterwards threads
+// call emit(col, n, sum) for the 16 * NV results.  Every thread must call.
+template <int NV, int NRED, typename Emit>
+__device__ __forceinline__ void col_reduce(double (&v)[NV], double (*s_red)[16][NRED], Emit emit) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int n = 0; n < NV; n++) {
+        double x = v[n] + __shfl_xor_sync(0xffffffffu, v[n], 16);
+        if (lane < 16) s_red[warp][lane][n] = x;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < 16 * NV; o += blockDim.x) {
+        int cc = o / NV, n = o % NV;
+        double s = 0;
+#pragma unroll
+        for (int w = 0; w < 8; w++) s += s_red[w][cc][n];
+        emit(cc, n, s);
+    }
+    __syncthreads();
+}
+
+template <int LI, int LJ, int LK, int LL, typename F>
+__global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
+    constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = ncart(LK), NFL = ncart(LL);
+    constexpr int NIJ = NFI * NFJ, NKL = NFK * NFL, NF = NIJ * NKL;
+    constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
+    constexpr int GSZ = (LI + 1) * (LJ + 1) * (LK + 1) * (LL + 1);
+    constexpr int NRED = imax(NKL, imax(NFI * NFL, NFI * NFK));
+    __shared__ double s_red[8][16][NRED];
+
+    // tile of this block
+    int r, c;
+    if (T.tile_prefix != nullptr) {
+        int lo = 0, hi = T.nrows - 1;
+        const int x = blockIdx.x;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (__ldg(T.tile_prefix + mid) <= x) lo = mid; else hi = mid - 1;
+        }
+        r = lo;
+        c = x - __ldg(T.tile_prefix + r);
+    } else {
+        int ncols = ((T.rows_are_b ? T.na : T.nb) + TILE - 1) / TILE;
+        r = blockIdx.x / ncols;
+        c = blockIdx.x % ncols;
+    }
+    const int ta = T.rows_are_b ? c : r, tb = T.rows_are_b ? r : c;
+    const int a_begin = T.a0 + ta * TILE, b_begin = T.b0 + tb * TILE;
+    const int a_end = min(T.a0 + T.na, a_begin + TILE), b_end = min(T.b0 + T.nb, b_begin + TILE);
+    if (T.diag && b_begin > a_end - 1) return;
+
+    const int row = threadIdx.x >> 4, col = threadIdx.x & 15;
+    const int a = a_begin + row, b = b_begin + col;
+    const bool row_ok = a < a_end, col_ok = b < b_end;
+    // shells shared across the tile
+    const int i_tile = __ldg(A.pair_bra + a_begin), k_tile = __ldg(A.pair_bra + b_begin);
+    const int ish = row_ok ? __ldg(A.pair_bra + a) : i_tile;
+    const int ksh = col_ok ? __ldg(A.pair_bra + b) : k_tile;
+    const bool bra_uni = __syncthreads_and(ish == i_tile);
+    const bool ket_uni = __syncthreads_and(ksh == k_tile);
+
+    bool active = row_ok && col_ok && (!T.diag || a >= b);
+    Quartet Q;
+    if (active) {
+        load_quartet(A, a, b, Q);
+        if (A.pair_q != nullptr) {
+            double bound = __ldg(A.pair_q + a) * __ldg(A.pair_q + b);
+            if (A.dm_cond != nullptr) bound *= dmax6(A.dm_cond, A.nbas, Q.ish, Q.jsh, Q.ksh, Q.lsh);
+            active = bound >= A.tol && (A.tol_hi <= 0. || bound < A.tol_hi);
+        }
+    }
+    if (!__syncthreads_or(active)) return;
+
+    F acc[NF];
+#pragma unroll
+    for (int n = 0; n < NF; n++) acc[n] = F(0);
+    if (active) {
+        F AB[3], CD[3];
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            AB[d] = F(Q.A[d] - Q.B[d]);
+            CD[d] = F(Q.C[d] - Q.D[d]);
+        }
+        const int pa = T.pa0 + (a - T.a0) * T.nprim_a;
+        const int pb = T.pb0 + (b - T.b0) * T.nprim_b;
+        for (int ip = 0; ip < T.nprim_a; ip++) {
+            for (int kp = 0; kp < T.nprim_b; kp++) {
+                PrimQuartet P;
+                load_prim(A, Q, pa + ip, pb + kp, P);
+                double rt[NR], wt[NR];
+                if constexpr (NR == 1) rys_roots1(P.x, rt[0], wt[0]);
+                else rys_roots<NR>(A.rys, P.x, rt, wt);
+#pragma unroll
+                for (int rr = 0; rr < NR; rr++) {
+                    RootCoef cf = root_coef(rt[rr], P.p, P.q, P.inv_pq);
+                    F g[3][GSZ];
+#pragma unroll
+                    for (int d = 0; d < 3; d++) {
+                        F seed = (d == 2) ? F(wt[rr] * P.pref) : F(1);
+                        gen_2d<LI, LJ, LK, LL, F>(seed, F(P.PA[d] - cf.qs * P.PQ[d]),
+                                                  F(P.QC[d] + cf.ps * P.PQ[d]), F(cf.b00),
+                                                  F(cf.b10), F(cf.b01), AB[d], CD[d], g[d]);
+                    }
+#pragma unroll
+                    for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                    for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                    for (int fk = 0; fk < NFK; fk++)
+#pragma unroll
+                    for (int fl = 0; fl < NFL; fl++) {
+                        constexpr int SJ = (LK + 1) * (LL + 1), SI = (LJ + 1) * SJ;
+                        const int ix = cart_pow(LI, fi, 0) * SI + cart_pow(LJ, fj, 0) * SJ +
+                                       cart_pow(LK, fk, 0) * (LL + 1) + cart_pow(LL, fl, 0);
+                        const int iy = cart_pow(LI, fi, 1) * SI + cart_pow(LJ, fj, 1) * SJ +
+                                       cart_pow(LK, fk, 1) * (LL + 1) + cart_pow(LL, fl, 1);
+                        const int iz = cart_pow(LI, fi, 2) * SI + cart_pow(LJ, fj, 2) * SJ +
+                                       cart_pow(LK, fk, 2) * (LL + 1) + cart_pow(LL, fl, 2);
+                        acc[((fi * NFJ + fj) * NFK + fk) * NFL + fl] += g[0][ix] * g[1][iy] * g[2][iz];
+                    }
+                }
+            }
+        }
+    }
+
+    // ---- digestion: one density block and one target at a time ----
+    const int nao = A.nao;
+    const size_t nn = (size_t)nao * nao;
+    const int i0t = __ldg(A.ao_loc + i_tile), k0t = __ldg(A.ao_loc + k_tile);
+#define ACC(fi, fj, fk, fl) ((double)acc[(((fi) * NFJ + (fj)) * NFK + (fk)) * NFL + (fl)])
+    for (int id = 0; id < A.n_dm; id++) {
+        const double *__restrict__ D = A.dm + id * nn;
+        auto ld = [&](int r0, int c0) { return __ldg(D + (size_t)r0 * nao + c0); };
+        if (A.vj != nullptr) {
+            double *VJ = A.vj + id * nn;
+            double pij[NIJ];
+#pragma unroll
+            for (int n = 0; n < NIJ; n++) pij[n] = 0;
+            if (active) {
+#pragma unroll
+                for (int kl = 0; kl < NKL; kl++) {
+                    const double d = ld(Q.k0 + kl / NFL, Q.l0 + kl % NFL);
+#pragma unroll
+                    for (int ij = 0; ij < NIJ; ij++) pij[ij] += (double)acc[ij * NKL + kl] * d;
+                }
+            }
+            row_reduce(pij);
+            if (col == 0 && row_ok) {
+                const int jr = __ldg(A.pair_ket + a);
+                const int i0 = __ldg(A.ao_loc + ish), j0 = __ldg(A.ao_loc + jr);
+#pragma unroll
+                for (int n = 0; n < NIJ; n++)
+                    if (pij[n] != 0) atomicAdd(VJ + (size_t)(i0 + n / NFJ) * nao + j0 + n % NFJ, pij[n]);
+            }
+            double pkl[NKL];
+#pragma unroll
+            for (int n = 0; n < NKL; n++) pkl[n] = 0;
+            if (active) {
+#pragma unroll
+                for (int ij = 0; ij < NIJ; ij++) {
+                    const double d = ld(Q.i0 + ij / NFJ, Q.j0 + ij % NFJ);
+#pragma unroll
+                    for (int kl = 0; kl < NKL; kl++) pkl[kl] += (double)acc[ij * NKL + kl] * d;
+                }
+            }
+            col_reduce<NKL, NRED>(pkl, s_red, [&](int cc, int n, double v) {
+                const int bb = b_begin + cc;
+                if (v != 0 && bb < b_end) {
+                    const int k0 = __ldg(A.ao_loc + __ldg(A.pair_bra + bb));
+                    const int l0 = __ldg(A.ao_loc + __ldg(A.pair_ket + bb));
+                    atomicAdd(VJ + (size_t)(k0 + n / NFL) * nao + l0 + n % NFL, v);
+                }
+            });
+        }
+        if (A.vk != nullptr) {
+            double *VK = A.vk + id * nn;
+            // K_jl = sum_ik (ij|kl) D_ik: one target per quartet
+            if (active) {
+                double pjl[NFJ * NFL];
+#pragma unroll
+                for (int n = 0; n < NFJ * NFL; n++) pjl[n] = 0;
+#pragma unroll
+                for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                    for (int fk = 0; fk < NFK; fk++) {
+                        const double d = ld(Q.i0 + fi, Q.k0 + fk);
+#pragma unroll
+                        for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                            for (int fl = 0; fl < NFL; fl++) pjl[fj * NFL + fl] += ACC(fi, fj, fk, fl) * d;
+                    }
+#pragma unroll
+                for (int n = 0; n < NFJ * NFL; n++)
+                    if (pjl[n] != 0) atomicAdd(VK + (size_t)(Q.j0 + n / NFL) * nao + Q.l0 + n % NFL, pjl[n]);
+            }
+            // K_jk = sum_il (ij|kl) D_il: shared k -> sum over the row
+            {
+                double pjk[NFJ * NFK];
+#pragma unroll
+                for (int n = 0; n < NFJ * NFK; n++) pjk[n] = 0;
+                if (active) {
+#pragma unroll
+                    for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                        for (int fl = 0; fl < NFL; fl++) {
+                            const double d = ld(Q.i0 + fi, Q.l0 + fl);
+#pragma unroll
+                            for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                                for (int fk = 0; fk < NFK; fk++) pjk[fj * NFK + fk] += ACC(fi, fj, fk, fl) * d;
+                        }
+                }
+                if (ket_uni) {
+                    row_reduce(pjk);
+                    if (col == 0 && row_ok) {
+                        const int j0 = __ldg(A.ao_loc + __ldg(A.pair_ket + a));
+#pragma unroll
+                        for (int n = 0; n < NFJ * NFK; n++)
+                            if (pjk[n] != 0) atomicAdd(VK + (size_t)(j0 + n / NFK) * nao + k0t + n % NFK, pjk[n]);
+                    }
+                } else if (active) {
+#pragma unroll
+                    for (int n = 0; n < NFJ * NFK; n++)
+                        if (pjk[n] != 0) atomicAdd(VK + (size_t)(Q.j0 + n / NFK) * nao + Q.k0 + n % NFK, pjk[n]);
+                }
+            }
+            // K_il = sum_jk (ij|kl) D_jk: shared i -> sum over the column
+            {
+                double pil[NFI * NFL];
+#pragma unroll
+                for (int n = 0; n < NFI * NFL; n++) pil[n] = 0;
+                if (active) {
+#pragma unroll
+                    for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                        for (int fk = 0; fk < NFK; fk++) {
+                            const double d = ld(Q.j0 + fj, Q.k0 + fk);
+#pragma unroll
+                            for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                                for (int fl = 0; fl < NFL; fl++) pil[fi * NFL + fl] += ACC(fi, fj, fk, fl) * d;
+                        }
+                }
+                if (bra_uni) {
+                    col_reduce<NFI * NFL, NRED>(pil, s_red, [&](int cc, int n, double v) {
+                        const int bb = b_begin + cc;
+                        if (v != 0 && bb < b_end) {
+                            const int l0 = __ldg(A.ao_loc + __ldg(A.pair_ket + bb));
+                            atomicAdd(VK + (size_t)(i0t + n / NFL) * nao + l0 + n % NFL, v);
+                        }
+                    });
+                } else if (active) {
+#pragma unroll
+                    for (int n = 0; n < NFI * NFL; n++)
+                        if (pil[n] != 0) atomicAdd(VK + (size_t)(Q.i0 + n / NFL) * nao + Q.l0 + n % NFL, pil[n]);
+                }
+            }
+            // K_ik = sum_jl (ij|kl) D_jl
+            {
+                double pik[NFI * NFK];
+#pragma unroll
+                for (int n = 0; n < NFI * NFK; n++) pik[n] = 0;
+                if (active) {
+#pragma unroll
+                    for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                        for (int fl = 0; fl < NFL; fl++) {
+                            const double d = ld(Q.j0 + fj, Q.l0 + fl);
+#pragma unroll
+                            for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                                for (int fk = 0; fk < NFK; fk++) pik[fi * NFK + fk] += ACC(fi, fj, fk, fl) * d;
+                        }
+                }
+                if (bra_uni && ket_uni) {
+                    row_reduce(pik);
+                    col_reduce<NFI * NFK, NRED>(pik, s_red, [&](int cc, int n, double v) {
+                        // after the row sums each column holds its row total, so
+                        // column 0 carries the sum over the whole tile
+                        if (cc == 0 && v != 0)
+                            atomicAdd(VK + (size_t)(i0t + n / NFK) * nao + k0t + n % NFK, v);
+                    });
+                } else if (bra_uni) {
+                    col_reduce<NFI * NFK, NRED>(pik, s_red, [&](int cc, int n, double v) {
+                        const int bb = b_begin + cc;
+                        if (v != 0 && bb < b_end) {
+                            const int k0 = __ldg(A.ao_loc + __ldg(A.pair_bra + bb));
+                            atomicAdd(VK + (size_t)(i0t + n / NFK) * nao + k0 + n % NFK, v);
+                        }
+                    });
+                } else if (ket_uni) {
+                    row_reduce(pik);
+                    if (col == 0 && row_ok) {
+                        const int i0 = __ldg(A.ao_loc + ish);
+#pragma unroll
+                        for (int n = 0; n < NFI * NFK; n++)
+                            if (pik[n] != 0) atomicAdd(VK + (size_t)(i0 + n / NFK) * nao + k0t + n % NFK, pik[n]);
+                    }
+                } else if (active) {
+#pragma unroll
+                    for (int n = 0; n < NFI * NFK; n++)
+                        if (pik[n] != 0) atomicAdd(VK + (size_t)(Q.i0 + n / NFK) * nao + Q.k0 + n % NFK, pik[n]);
+                }
+            }
+        }
+    }
+#undef ACC
+}
+
 // ---------------------------------------------------------------------------
 // group-per-quartet kernel
 template <int LI, int LJ, int LK, int LL, int NSPLIT>
@@ -341,7 +673,7 @@ struct GroupCfg {
     static constexpr size_t SMEM = (size_t)NG * PER_GROUP * sizeof(double);
 };
 
-template <int LI, int LJ, int LK, int LL, int NSPLIT>
+template <int LI, int LJ, int LK, int LL, int NSPLIT, typename F>
 __global__ void __launch_bounds__(GroupCfg<LI, LJ, LK, LL, NSPLIT>::NT)
 jk_group(JKArgs A, JKTask T) {
     using C = GroupCfg<LI, LJ, LK, LL, NSPLIT>;
@@ -359,6 +691,7 @@ jk_group(JKArgs A, JKTask T) {
     double *gbuf = smem + (in_group ? g : 0) * C::PER_GROUP;   // RB: g tables / reduction
     double *dbuf = gbuf + C::RB;                                // density blocks
     double *rw = dbuf + C::DBUF;                                // roots, weights
+    F *gtab = reinterpret_cast<F *>(gbuf);                      // per-root 2D tables
     double *Dij = dbuf, *Dkl = Dij + C::NIJ, *Dik = Dkl + C::NKL, *Dil = Dik + NFI * NFK;
     double *Djk = Dil + NFI * NFL, *Djl = Djk + NFJ * NFK;
 
@@ -395,9 +728,9 @@ jk_group(JKArgs A, JKTask T) {
             pa = T.pa0 + (Q.a - T.a0) * T.nprim_a;
             pb = T.pb0 + (Q.b - T.b0) * T.nprim_b;
         }
-        double acc[C::NACC];
+        F acc[C::NACC];
 #pragma unroll
-        for (int n = 0; n < C::NACC; n++) acc[n] = 0.0;
+        for (int n = 0; n < C::NACC; n++) acc[n] = F(0);
 
         for (int ip = 0; ip < T.nprim_a; ip++) {
             for (int kp = 0; kp < T.nprim_b; kp++) {
@@ -412,21 +745,21 @@ jk_group(JKArgs A, JKTask T) {
                         int r = task / 3, d = task % 3;
                         RootCoef c = root_coef(rw[r], P.p, P.q, P.inv_pq);
                         double seed = (d == 2) ? rw[NR + r] * P.pref : 1.0;
-                        gen_2d<LI, LJ, LK, LL, double>(seed, P.PA[d] - c.qs * P.PQ[d],
-                                                       P.QC[d] + c.ps * P.PQ[d], c.b00, c.b10,
-                                                       c.b01, AB[d], CD[d],
-                                                       gbuf + (d * NR + r) * GSZ);
+                        gen_2d<LI, LJ, LK, LL, F>(F(seed), F(P.PA[d] - c.qs * P.PQ[d]),
+                                                  F(P.QC[d] + c.ps * P.PQ[d]), F(c.b00), F(c.b10),
+                                                  F(c.b01), F(AB[d]), F(CD[d]),
+                                                  gtab + (d * NR + r) * GSZ);
                     }
                 }
                 __syncthreads();
                 if (active && lane < TPQ) {
 #pragma unroll
                     for (int r = 0; r < NR; r++) {
-                        const double *gx = gbuf + offx + r * GSZ;
-                        const double *gy = gbuf + offy + r * GSZ;
-                        const double *gz = gbuf + offz + r * GSZ;
+                        const F *gx = gtab + offx + r * GSZ;
+                        const F *gy = gtab + offy + r * GSZ;
+                        const F *gz = gtab + offz + r * GSZ;
                         if constexpr (NSPLIT == 1) {
-                            double xs[C::KLS], ys[C::KLS], zs[C::KLS];
+                            F xs[C::KLS], ys[C::KLS], zs[C::KLS];
 #pragma unroll
                             for (int u = 0; u < C::KLS; u++) {
                                 xs[u] = gx[u];
@@ -451,9 +784,9 @@ jk_group(JKArgs A, JKTask T) {
 #pragma unroll
                                     for (int c = 0; c < NFK; c++)
                                         if (c == fk) { kx = cart_pow(LK, c, 0); ky = cart_pow(LK, c, 1); kz = cart_pow(LK, c, 2); }
-                                    const double *rx = gx + kx * (LL + 1);
-                                    const double *ry = gy + ky * (LL + 1);
-                                    const double *rz = gz + kz * (LL + 1);
+                                    const F *rx = gx + kx * (LL + 1);
+                                    const F *ry = gy + ky * (LL + 1);
+                                    const F *rz = gz + kz * (LL + 1);
 #pragma unroll
                                     for (int fl = 0; fl < NFL; fl++) {
                                         acc[ck * NFL + fl] = fma(rx[cart_pow(LL, fl, 0)] * ry[cart_pow(LL, fl, 1)],
@@ -493,7 +826,7 @@ jk_group(JKArgs A, JKTask T) {
                     int fk = chunk * CK + ck;
                     if (fk < NFK) {
 #pragma unroll
-                        for (int fl = 0; fl < NFL; fl++) s = fma(acc[ck * NFL + fl], Dkl[fk * NFL + fl], s);
+                        for (int fl = 0; fl < NFL; fl++) s = fma((double)acc[ck * NFL + fl], Dkl[fk * NFL + fl], s);
                     }
                 }
                 atomicAdd(A.vj + id * nn + (size_t)(Q.i0 + fi) * nao + Q.j0 + fj, s);
@@ -512,8 +845,8 @@ jk_group(JKArgs A, JKTask T) {
                             double sik = 0, sjk = 0;
 #pragma unroll
                             for (int fl = 0; fl < NFL; fl++) {
-                                sik = fma(acc[ck * NFL + fl], Djl[fj * NFL + fl], sik);
-                                sjk = fma(acc[ck * NFL + fl], Dil[fi * NFL + fl], sjk);
+                                sik = fma((double)acc[ck * NFL + fl], Djl[fj * NFL + fl], sik);
+                                sjk = fma((double)acc[ck * NFL + fl], Dil[fi * NFL + fl], sjk);
                             }
                             Sik[(fi * NFK + fk) * NFJ + fj] = sik;
                             Sjk[(fj * NFK + fk) * NFI + fi] = sjk;
@@ -526,8 +859,8 @@ jk_group(JKArgs A, JKTask T) {
                         for (int ck = 0; ck < CK; ck++) {
                             int fk = chunk * CK + ck;
                             if (fk < NFK) {
-                                sil = fma(acc[ck * NFL + fl], Djk[fj * NFK + fk], sil);
-                                sjl = fma(acc[ck * NFL + fl], Dik[fi * NFK + fk], sjl);
+                                sil = fma((double)acc[ck * NFL + fl], Djk[fj * NFK + fk], sil);
+                                sjl = fma((double)acc[ck * NFL + fl], Dik[fi * NFK + fk], sjl);
                             }
                         }
                         Sil[((fi * NFL + fl) * NFJ + fj) * NSPLIT + chunk] = sil;
@@ -576,7 +909,7 @@ jk_group(JKArgs A, JKTask T) {
                             if (fk >= fk0 && fk < fk0 + C::FKB && fk < NFK) {
 #pragma unroll
                                 for (int fl = 0; fl < NFL; fl++)
-                                    Sj[((fk - fk0) * NFL + fl) * C::NIJ + fij] = acc[ck * NFL + fl] * dij;
+                                    Sj[((fk - fk0) * NFL + fl) * C::NIJ + fij] = (double)acc[ck * NFL + fl] * dij;
                             }
                         }
                     }
@@ -609,14 +942,14 @@ static int launch_small(const JKArgs &args, const JKTask &task, int fp32, cudaSt
     int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
     if (ntiles == 0) return 0;
     if (fp32)
-        jk_small<LI, LJ, LK, LL, float><<<ntiles, 256, 0, stream>>>(args, task);
+        jk_tile<LI, LJ, LK, LL, float><<<ntiles, 256, 0, stream>>>(args, task);
     else
-        jk_small<LI, LJ, LK, LL, double><<<ntiles, 256, 0, stream>>>(args, task);
+        jk_tile<LI, LJ, LK, LL, double><<<ntiles, 256, 0, stream>>>(args, task);
     return 0;
 }
 
-template <int LI, int LJ, int LK, int LL, int NSPLIT>
-static int launch_group(const JKArgs &args, const JKTask &task, cudaStream_t stream) {
+template <int LI, int LJ, int LK, int LL, int NSPLIT, typename F>
+static int launch_group_f(const JKArgs &args, const JKTask &task, cudaStream_t stream) {
     using C = GroupCfg<LI, LJ, LK, LL, NSPLIT>;
     static_assert(C::SMEM + 2048 <= 227 * 1024, "shared memory per CTA");
     static_assert(C::NT <= 1024, "threads per CTA");
@@ -624,12 +957,18 @@ static int launch_group(const JKArgs &args, const JKTask &task, cudaStream_t str
     if (ntiles == 0) return 0;
     static bool configured = false;
     if (!configured) {
-        cudaFuncSetAttribute(jk_group<LI, LJ, LK, LL, NSPLIT>,
+        cudaFuncSetAttribute(jk_group<LI, LJ, LK, LL, NSPLIT, F>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
         configured = true;
     }
-    jk_group<LI, LJ, LK, LL, NSPLIT><<<ntiles, C::NT, C::SMEM, stream>>>(args, task);
+    jk_group<LI, LJ, LK, LL, NSPLIT, F><<<ntiles, C::NT, C::SMEM, stream>>>(args, task);
     return 0;
+}
+
+template <int LI, int LJ, int LK, int LL, int NSPLIT>
+static int launch_group(const JKArgs &args, const JKTask &task, int fp32, cudaStream_t stream) {
+    if (fp32) return launch_group_f<LI, LJ, LK, LL, NSPLIT, float>(args, task, stream);
+    return launch_group_f<LI, LJ, LK, LL, NSPLIT, double>(args, task, stream);
 }
 
 // Bra side = pair (LI, LJ) (threads), ket side = pair (LK, LL) (accumulators).
@@ -643,7 +982,7 @@ static int launch_class(const JKArgs &args, const JKTask &task, int fp32, cudaSt
         return launch_small<L1, L2, L3, L4>(args, task, fp32, stream);
     } else if constexpr (N12 <= N34) {
         constexpr int NS = cdiv(N34, 36) > ncart(L3) ? ncart(L3) : cdiv(N34, 36);
-        return launch_group<L1, L2, L3, L4, NS>(args, task, stream);
+        return launch_group<L1, L2, L3, L4, NS>(args, task, fp32, stream);
     } else {
         constexpr int NS = cdiv(N12, 36) > ncart(L1) ? ncart(L1) : cdiv(N12, 36);
         JKTask sw = task;
@@ -651,7 +990,7 @@ static int launch_class(const JKArgs &args, const JKTask &task, int fp32, cudaSt
         sw.pa0 = task.pb0; sw.pb0 = task.pa0; sw.nprim_a = task.nprim_b; sw.nprim_b = task.nprim_a;
         sw.rows_are_b = !task.rows_are_b;
         // diag tasks have identical lists on both sides; the a >= b rule stays
-        return launch_group<L3, L4, L1, L2, NS>(args, sw, stream);
+        return launch_group<L3, L4, L1, L2, NS>(args, sw, fp32, stream);
     }
 }
 

@@ -106,6 +106,53 @@ def _make_s_index_offsets(log_q, nbins=10, cutoff=1e-12):
     return np.append(0, np.cumsum(bins)).astype(np.int32)
 
 
+PAIR_TILE = 16
+
+
+def _tile_order(bra, ket, q):
+    """Order the pairs of one class in tiles of PAIR_TILE pairs that share the
+    bra shell: pairs are grouped by bra shell, sorted by q descending within a
+    group, cut into tiles (the last tile of a group padded with pairs of
+    q = 0), and the tiles are sorted by their largest q.  So q is descending
+    within a tile and the first q of every tile is descending along the list,
+    which keeps the tile pruning of BQCbuild_jk valid, and a J/K kernel can
+    reduce the contributions that share a shell across a tile.  Returns
+    (bra, ket, q, is_padding)."""
+    n = len(q)
+    if n == 0:
+        return bra, ket, q, np.zeros(0, bool)
+    order = np.lexsort((-q, bra))
+    b, k, qq = bra[order], ket[order], q[order]
+    starts = np.flatnonzero(np.r_[True, b[1:] != b[:-1]])
+    sizes = np.diff(np.r_[starts, n])
+    gid = np.repeat(np.arange(len(starts)), sizes)
+    rank = np.arange(n) - starts[gid]
+    ntile_g = (sizes + PAIR_TILE - 1) // PAIR_TILE
+    tile_off = np.r_[0, np.cumsum(ntile_g)[:-1]]
+    tile = tile_off[gid] + rank // PAIR_TILE
+    slot = rank % PAIR_TILE
+    ntile = int(ntile_g.sum())
+    first = slot == 0
+    tq = np.empty(ntile)
+    tq[tile[first]] = qq[first]
+    tb = np.empty(ntile, dtype=b.dtype)
+    tb[tile[first]] = b[first]
+    tk = np.empty(ntile, dtype=k.dtype)
+    tk[tile[first]] = k[first]
+    pos = np.empty(ntile, dtype=np.int64)
+    pos[np.argsort(-tq, kind='stable')] = np.arange(ntile)
+    out_b = np.repeat(tb[np.argsort(pos)], PAIR_TILE)
+    out_k = np.repeat(tk[np.argsort(pos)], PAIR_TILE)
+    out_q = np.zeros(ntile * PAIR_TILE)
+    dummy = np.ones(ntile * PAIR_TILE, bool)
+    dst = pos[tile] * PAIR_TILE + slot
+    out_b[dst] = b
+    out_k[dst] = k
+    out_q[dst] = qq
+    dummy[dst] = False
+    return out_b, out_k, out_q, dummy
+
+
 class _VHFOpt:
     """Basis sort, Schwarz pair lists and the device basis-product cache.
 
@@ -126,7 +173,7 @@ class _VHFOpt:
         self._bp_gpu = None
 
     # -- helpers ---------------------------------------------------------------
-    def _init_cache(self, pair2shls, pairs_locs, ncptype, diag_fac):
+    def _init_cache(self, pair2shls, pairs_locs, ncptype, diag_fac, dummy=None):
         lib = _libmod.load_library()
         mol = self.mol
         bp_cpu = ctypes.POINTER(_libmod.BasisProdCache)()
@@ -145,6 +192,17 @@ class _VHFOpt:
             env.ctypes.data_as(ctypes.c_void_p))
         nprim = bp_cpu.contents.primitive_pairs_locs[ncptype]
         aexyz = np.ctypeslib.as_array(bp_cpu.contents.aexyz, (max(nprim, 1) * 5,)).copy()
+        if dummy is not None and dummy.any():
+            # padding pairs contribute exactly zero: e12 = 0 for all their primitives
+            e12 = aexyz[nprim:2 * nprim]
+            for c in range(ncptype):
+                p0, p1 = pairs_locs[c], pairs_locs[c + 1]
+                d = np.flatnonzero(dummy[p0:p1])
+                if len(d):
+                    n12 = bp_cpu.contents.cptype[c].nprim_12
+                    base = bp_cpu.contents.primitive_pairs_locs[c]
+                    idx = (base + d[:, None] * n12 + np.arange(n12)[None, :]).ravel()
+                    e12[idx] = 0.
         dev = _dev()
         mem = {
             'ao_loc': torch.as_tensor(mol.ao_loc_nr(cart=True), dtype=torch.int32, device=dev),
@@ -216,23 +274,28 @@ class _VHFOpt:
         self._free_cache(bp_cpu, bp_gpu)
         del mem, keep
 
-        # pass 2: keep q > cutoff, sorted descending per class
-        pair2bra, pair2ket, qs, log_qs = [], [], [], []
+        # pass 2: keep q > cutoff and lay every class out in tiles of 16 pairs
+        # sharing the bra shell (see _tile_order)
+        pair2bra, pair2ket, qs, log_qs, dummies = [], [], [], [], []
         for c in range(ncptype):
             q = q_all[locs[c]:locs[c + 1]]
-            order = np.argsort(-q, kind='stable')
-            order = order[q[order] > cutoff]
-            pair2bra.append(p2s[0, locs[c]:locs[c + 1]][order])
-            pair2ket.append(p2s[1, locs[c]:locs[c + 1]][order])
-            qs.append(q[order])
-            lq = np.log(q[order]) if len(order) else np.zeros(0)
+            keep = q > cutoff
+            b, k, q = p2s[0, locs[c]:locs[c + 1]][keep], p2s[1, locs[c]:locs[c + 1]][keep], q[keep]
+            b, k, q, dummy = _tile_order(b, k, q)
+            pair2bra.append(b)
+            pair2ket.append(k)
+            qs.append(q)
+            dummies.append(dummy)
+            with np.errstate(divide='ignore'):
+                lq = np.log(np.maximum(q, cutoff)) if len(q) else np.zeros(0)
             log_qs.append(np.minimum(lq, 0))
         self.log_qs = log_qs
         self.bas_pairs_locs = np.append(0, np.cumsum([len(x) for x in pair2bra])).astype(np.int32)
         self.bas_pair2shls = np.vstack([np.hstack(pair2bra), np.hstack(pair2ket)]).astype(np.int32)
+        self.pair_dummy = np.hstack(dummies) if dummies else np.zeros(0, bool)
         self.ncptype = ncptype
         self._bp_cpu, self._bp_gpu, self._mem, self._keep = self._init_cache(
-            self.bas_pair2shls, self.bas_pairs_locs, ncptype, scale_diag)
+            self.bas_pair2shls, self.bas_pairs_locs, ncptype, scale_diag, self.pair_dummy)
         self.pair_q_host = np.ascontiguousarray(np.hstack(qs) if qs else np.zeros(1))
         self.pair_q = torch.as_tensor(self.pair_q_host, device=_dev())
         self.coeff_dev = torch.as_tensor(self.coeff, device=_dev())
@@ -474,10 +537,19 @@ class RHF(_SCFBase):
     ``kernel()`` returns the total energy (pyscf convention).  Convergence is
     |Delta E| < conv_tol; incremental (difference-density) Fock builds as in
     pyscf's direct SCF, with a full rebuild every ``rebuild_cycle`` cycles.
+
+    Mixed precision (``fp32_threshold > 0``): on the incremental builds the
+    quartets whose bound q_ij q_kl max|dD| is below fp32_threshold are
+    evaluated in FP32 (roots, weights, Fock accumulation stay FP64); once
+    |Delta E| < ``mixed_switch_tol`` every further cycle is a full FP64
+    rebuild, and convergence is only accepted between two such cycles, so
+    the converged energy is an FP64 energy.
     """
 
     rebuild_cycle = 8
-    jk_hook = None   # optional callable(density) run after each J/K build (accounting)
+    fp32_threshold = 0.
+    mixed_switch_tol = 1e-6
+    jk_hook = None   # optional callable(density, fp32_below) run after each J/K build
 
     def init_guess_dm(self):
         from .guess import init_guess
@@ -508,28 +580,40 @@ class RHF(_SCFBase):
         dm_last = None
         e_last = None
         self.converged = False
+        mixed = self.fp32_threshold > 0
+        final = not mixed          # in the final (all-FP64) phase
+        n_final = 0
         t_jk = 0.
+        self.build_log = []
         for cycle in range(self.max_cycle):
             tj = time.perf_counter()
-            if dm_last is None or cycle % self.rebuild_cycle == 0:
+            full = dm_last is None or cycle % self.rebuild_cycle == 0 or (mixed and final)
+            fp32_below = 0. if (final or full) else self.fp32_threshold
+            if full:
                 dm_in = dm
                 vj, vk = opt.jk_ao(dm[None])
             else:
                 dm_in = dm - dm_last
-                dvj, dvk = opt.jk_ao(dm_in[None])
+                dvj, dvk = opt.jk_ao(dm_in[None], fp32_below=fp32_below)
                 vj = vj + dvj
                 vk = vk + dvk
             torch.cuda.synchronize()
             t_jk += time.perf_counter() - tj
+            self.build_log.append(('full' if full else 'incr', fp32_below))
             if self.jk_hook is not None:
-                self.jk_hook(dm_in)
+                self.jk_hook(dm_in, fp32_below)
             F = h + vj[0] - .5 * vk[0]
             e = float(.5 * torch.sum(dm * (h + F))) + e_nuc
             self.cycles = cycle + 1
-            if e_last is not None and abs(e - e_last) < self.conv_tol:
+            if final:
+                n_final += 1
+            de = abs(e - e_last) if e_last is not None else float('inf')
+            if de < self.conv_tol and final and (not mixed or n_final >= 2):
                 self.converged = True
                 self.e_tot = e
                 break
+            if mixed and not final and de < self.mixed_switch_tol:
+                final = True
             e_last = e
             err = F @ dm @ S - S @ dm @ F
             Fd = self._diis(F, err)

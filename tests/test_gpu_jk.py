@@ -82,10 +82,12 @@ def test_schwarz_and_int1e(cuda):
     assert abs(V - rV).max() < 1e-10
     # Schwarz factors of the kept pairs against the oracle's (ij|ij)
     q = oracle.q_cond(opt.mol)
-    p2s = opt.bas_pair2shls
-    dev_q = opt.pair_q.cpu().numpy()
+    real = ~opt.pair_dummy          # padding pairs of the tile layout carry q = 0
+    p2s = opt.bas_pair2shls[:, real]
+    dev_q = opt.pair_q.cpu().numpy()[real]
     ref = q[p2s[0], p2s[1]]
     assert np.allclose(dev_q, ref, rtol=1e-10, atol=1e-14)
+    assert (opt.pair_q.cpu().numpy()[~real] == 0).all()
 
 
 def test_gint_abi_matches_native(cuda):
@@ -104,14 +106,17 @@ def test_gint_abi_matches_native(cuda):
     nao = dmc.shape[-1]
     vj = torch.zeros_like(dmc)
     vk = torch.zeros_like(dmc)
-    nbins = 10
+    # the native pair lists are laid out in shell-grouped tiles (q is not
+    # globally sorted, padding pairs are interleaved), so drive GINTbuild_jk
+    # with one bin that spans each whole class
+    nbins = 1
     stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
     for cij in range(opt.ncptype):
         for ckl in range(cij + 1):
             if len(opt.log_qs[cij]) == 0 or len(opt.log_qs[ckl]) == 0:
                 continue
-            bi = hf._make_s_index_offsets(opt.log_qs[cij], nbins, opt.direct_scf_tol)
-            bk = hf._make_s_index_offsets(opt.log_qs[ckl], nbins, opt.direct_scf_tol)
+            bi = np.array([0, len(opt.log_qs[cij])], dtype=np.int32)
+            bk = np.array([0, len(opt.log_qs[ckl])], dtype=np.int32)
             err = lib.GINTbuild_jk(opt.bpcache, ctypes.c_void_p(vj.data_ptr()),
                                    ctypes.c_void_p(vk.data_ptr()), ctypes.c_void_p(dmc.data_ptr()),
                                    ctypes.c_int(nao), ctypes.c_int(1),
@@ -124,9 +129,8 @@ def test_gint_abi_matches_native(cuda):
     J = (C.T @ J[0] @ C).cpu().numpy()
     K = (C.T @ K[0] @ C).cpu().numpy()
     rj, rk = oracle.get_jk(mol, dm)
-    # bins drop quartets below the Schwarz-only bound, so agreement is to ~tol
-    assert abs(J - rj).max() < 1e-8
-    assert abs(K - rk).max() < 1e-8
+    assert abs(J - rj).max() < 1e-9
+    assert abs(K - rk).max() < 1e-9
 
 
 def test_rhf_energy(cuda):
@@ -157,3 +161,38 @@ def test_alkane_631gss(cuda):
     rj, rk = oracle.get_jk(mol, dm)
     assert abs(vj - rj).max() < TOL_JK * 10
     assert abs(vk - rk).max() < TOL_JK * 10
+
+
+def test_mixed_precision_jk_error(cuda):
+    """FP32 band below 1e-6: J/K error against the FP64 build stays small."""
+    import torch
+    from byteqc_b200.scf import hf
+    mol = _mol('cc-pvtz', nw=2, seed=5)
+    opt = hf._VHFOpt(mol).build()
+    rng = np.random.default_rng(8)
+    dm = rng.random((mol.nao, mol.nao)) * 1e-3
+    dm = torch.as_tensor(dm + dm.T, device=cuda)[None]
+    vj0, vk0 = opt.jk_ao(dm)
+    vj1, vk1 = opt.jk_ao(dm, fp32_below=1e-6)
+    ej = float((vj1 - vj0).abs().max())
+    ek = float((vk1 - vk0).abs().max())
+    assert ej < 1e-9 and ek < 1e-9, (ej, ek)
+    # every quartet is in the FP32 band: still within FP32 accuracy of FP64
+    vj2, vk2 = opt.jk_ao(dm, fp32_below=1e30)
+    assert float((vj2 - vj0).abs().max()) < 1e-5 * float(vj0.abs().max())
+    assert float((vk2 - vk0).abs().max()) < 1e-5 * float(vk0.abs().max())
+
+
+def test_mixed_precision_scf_energy(cuda):
+    from byteqc_b200.scf import hf
+    mol = _mol('cc-pvdz', nw=3, seed=4)
+    mf0 = hf.RHF(mol)
+    mf0.conv_tol = 1e-10
+    e0 = mf0.kernel()
+    mf1 = hf.RHF(mol)
+    mf1.conv_tol = 1e-10
+    mf1.fp32_threshold = 1e-6
+    e1 = mf1.kernel()
+    assert mf0.converged and mf1.converged
+    assert abs(e1 - e0) < 1e-9
+    assert any(f > 0 for kind, f in mf1.build_log)
