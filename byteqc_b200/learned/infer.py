@@ -1,0 +1,37 @@
+"""Initial density from the trained MLP (SAD plus predicted pair blocks)."""
+import os
+
+import numpy as np
+import torch
+
+from . import dataset
+from .model import DensityMLP
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_WEIGHTS = os.path.join(HERE, 'weights_ccpvdz.npz')
+_MODELS = {}
+
+
+def load_model(path=DEFAULT_WEIGHTS):
+    if path not in _MODELS:
+        if not os.path.exists(path):
+            raise FileNotFoundError('no trained density model at %s' % path)
+        _MODELS[path] = DensityMLP().load(dict(np.load(path)))
+    return _MODELS[path]
+
+
+def mlp_density(mf, dm_sad=None, path=DEFAULT_WEIGHTS):
+    """Predicted AO density (device tensor) for the molecule of mf."""
+    from ..scf.guess import init_guess
+    mol = mf.mol
+    if dm_sad is None:
+        dm_sad = init_guess(mf, 'sad')
+    model = load_model(path)
+    pf = dataset.pair_frames(mol)
+    pred = model.predict(pf.feats).cpu().numpy().astype(np.float64)
+    dm = dataset.assemble(mol, pf, pred, dm_sad.cpu().numpy())
+    dm = torch.as_tensor(dm, device=dm_sad.device)
+    ne = float(torch.sum(dm * mf.get_ovlp()))
+    if ne > 0:
+        dm *= mol.nelectron / ne
+    return dm

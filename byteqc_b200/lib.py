@@ -17,7 +17,8 @@ _lib = None
 SYMBOLS = ('GINTinit_basis_prod_cpu', 'GINTinit_basis_prod_gpu', 'GINTdel_basis_prod',
            'GINTbuild_jk', 'BQCbuild_jk', 'BQCbuild_jk_class', 'BQCcount_quartets',
            'BQCfp64_fma_peak', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e', 'BQClaunch_counter',
-           'BQCbuild_jk_noalloc', 'BQCversion')
+           'BQCbuild_jk_noalloc', 'BQCmlp_linear_fwd', 'BQCmlp_linear_bwd', 'BQCmlp_adam',
+           'BQCmlp_to_bf16', 'BQCversion')
 
 
 def load_library(name='libbyteqc_b200'):
@@ -45,6 +46,11 @@ def load_library(name='libbyteqc_b200'):
         [ctypes.c_void_p] * 3 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                                  ctypes.c_void_p]
     lib.BQCbuild_jk_noalloc.restype = ctypes.c_int
+    vp, ci, cf = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
+    lib.BQCmlp_linear_fwd.argtypes = [vp] * 6 + [ci] * 4 + [vp]
+    lib.BQCmlp_linear_bwd.argtypes = [vp] * 8 + [ci] * 3 + [vp]
+    lib.BQCmlp_adam.argtypes = [vp] * 5 + [ci, cf, cf, cf, cf, ci, vp]
+    lib.BQCmlp_to_bf16.argtypes = [vp, vp, ctypes.c_size_t, vp]
     lib.GINTinit_basis_prod_cpu.restype = None
     lib.GINTinit_basis_prod_gpu.restype = None
     lib.GINTdel_basis_prod.restype = None

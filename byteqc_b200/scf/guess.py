@@ -73,6 +73,9 @@ def init_guess(mf, kind='sad'):
         nocc = mol.nelectron // 2
         c = c[:, torch.argsort(e)[:nocc]]
         return 2. * c @ c.T
+    if kind == 'mlp':
+        from ..learned.infer import mlp_density, DEFAULT_WEIGHTS
+        return mlp_density(mf, init_guess(mf, 'sad'), getattr(mf, 'mlp_weights', DEFAULT_WEIGHTS))
     if kind not in ('sad', 'minao', 'atom'):
         raise ValueError('unknown init_guess %r' % kind)
     nao = mol.nao

@@ -392,11 +392,15 @@ class _VHFOpt:
 
 
 def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True, omega=None,
-           verbose=None, group_size=None, gpus=None, prescreen=True, nbins=None):
+           verbose=None, group_size=None, gpus=None, prescreen=True, nbins=None, fp32_below=0.,
+           tol=None):
     """Coulomb and exchange matrices for symmetric densities (host arrays in/out).
 
     Same signature and return convention as cuobc/scf/hf.py:53-227.
     ``prescreen=False`` disables the density screening (Schwarz only).
+    ``fp32_below`` (an addition, default 0 = all FP64) evaluates the quartets
+    whose bound q_ij q_kl max|D| is below it in FP32; ``tol`` (an addition)
+    overrides the screening threshold of vhfopt.
     """
     if hermi != 1:
         raise NotImplementedError('JK-builder only supports hermitian density matrix')
@@ -408,7 +412,7 @@ def get_jk(mol, dm, hermi=1, vhfopt=None, with_j=True, with_k=True, omega=None,
     nao0 = vhfopt.coeff.shape[1]
     dms = torch.as_tensor(dm0, dtype=torch.float64, device=_dev()).reshape(-1, nao0, nao0)
     if prescreen:
-        vj, vk = vhfopt.jk_ao(dms, with_j, with_k)
+        vj, vk = vhfopt.jk_ao(dms, with_j, with_k, fp32_below=fp32_below, tol=tol)
     else:
         C = vhfopt.coeff_dev
         dmc = torch.matmul(torch.matmul(C, dms), C.T)
@@ -536,19 +540,24 @@ class RHF(_SCFBase):
 
     ``kernel()`` returns the total energy (pyscf convention).  Convergence is
     |Delta E| < conv_tol; incremental (difference-density) Fock builds as in
-    pyscf's direct SCF, with a full rebuild every ``rebuild_cycle`` cycles.
+    pyscf's direct SCF (a full rebuild every ``rebuild_cycle`` cycles when it
+    is positive; by default only the first build is a full one).
 
     Mixed precision (``fp32_threshold > 0``): on the incremental builds the
     quartets whose bound q_ij q_kl max|dD| is below fp32_threshold are
-    evaluated in FP32 (roots, weights, Fock accumulation stay FP64); once
-    |Delta E| < ``mixed_switch_tol`` every further cycle is a full FP64
-    rebuild, and convergence is only accepted between two such cycles, so
-    the converged energy is an FP64 energy.
+    evaluated in FP32 (roots, weights, Fock accumulation stay FP64), and with
+    ``early_tol`` > direct_scf_tol those builds also drop quartets below
+    early_tol.  Once |Delta E| < ``mixed_switch_tol`` the Fock matrix is
+    rebuilt in full in FP64 at direct_scf_tol and the remaining cycles are
+    FP64 incremental builds at direct_scf_tol; convergence is only accepted
+    between two such final cycles, so the converged energy is an FP64 energy.
     """
 
-    rebuild_cycle = 8
+    rebuild_cycle = 0
     fp32_threshold = 0.
     mixed_switch_tol = 1e-6
+    early_tol = 0.
+    guess_fallback = False   # set when a learned guess was abandoned for SAD
     jk_hook = None   # optional callable(density, fp32_below) run after each J/K build
 
     def init_guess_dm(self):
@@ -587,19 +596,24 @@ class RHF(_SCFBase):
         self.build_log = []
         for cycle in range(self.max_cycle):
             tj = time.perf_counter()
-            full = dm_last is None or cycle % self.rebuild_cycle == 0 or (mixed and final)
+            full = dm_last is None or (self.rebuild_cycle > 0 and cycle % self.rebuild_cycle == 0) \
+                or (mixed and final and n_final == 0)
             fp32_below = 0. if (final or full) else self.fp32_threshold
+            tol = opt.direct_scf_tol
+            if mixed and not final and not full:
+                tol = max(tol, self.early_tol)
             if full:
                 dm_in = dm
                 vj, vk = opt.jk_ao(dm[None])
             else:
                 dm_in = dm - dm_last
-                dvj, dvk = opt.jk_ao(dm_in[None], fp32_below=fp32_below)
+                dvj, dvk = opt.jk_ao(dm_in[None], fp32_below=fp32_below, tol=tol)
                 vj = vj + dvj
                 vk = vk + dvk
             torch.cuda.synchronize()
-            t_jk += time.perf_counter() - tj
-            self.build_log.append(('full' if full else 'incr', fp32_below))
+            dt = time.perf_counter() - tj
+            t_jk += dt
+            self.build_log.append(('full' if full else 'incr', fp32_below, round(dt, 4)))
             if self.jk_hook is not None:
                 self.jk_hook(dm_in, fp32_below)
             F = h + vj[0] - .5 * vk[0]
@@ -616,6 +630,19 @@ class RHF(_SCFBase):
                 final = True
             e_last = e
             err = F @ dm @ S - S @ dm @ F
+            enorm = float(torch.linalg.norm(err))
+            if self.init_guess == 'mlp' and cycle == 1 and not self.guess_fallback \
+                    and enorm > self._enorm0:
+                # the DIIS error rose from the learned guess: restart from SAD
+                from .guess import init_guess
+                self.guess_fallback = True
+                self._diis_reset()
+                dm = init_guess(self, 'sad')
+                dm_last = None
+                e_last = None
+                continue
+            if cycle == 0:
+                self._enorm0 = enorm
             Fd = self._diis(F, err)
             mo_e, mo_c = self._eigh(Fd, S)
             occ = self.get_occ(mo_e)
@@ -650,20 +677,32 @@ class RHF(_SCFBase):
         e_last = None
         vj = vk = dm_last = None
         self.converged = False
+        mixed = self.fp32_threshold > 0
+        final = not mixed
+        n_final = 0
         for cycle in range(self.max_cycle):
-            if dm_last is None or cycle % self.rebuild_cycle == 0:
-                vj, vk = self.get_jk(self.mol, dm)
+            full = dm_last is None or (self.rebuild_cycle > 0 and cycle % self.rebuild_cycle == 0) \
+                or (mixed and final and n_final == 0)
+            if full:
+                vj, vk = get_jk(self.mol, dm, 1, self.opt)
             else:
-                dvj, dvk = self.get_jk(self.mol, dm - dm_last)
+                dvj, dvk = get_jk(self.mol, dm - dm_last, 1, self.opt,
+                                  fp32_below=0. if final else self.fp32_threshold,
+                                  tol=None if final else max(self.opt.direct_scf_tol, self.early_tol))
                 vj, vk = vj + dvj, vk + dvk
             h2d += dm.nbytes
             d2h += 2 * dm.nbytes
             F = h + vj - .5 * vk
             e = float(.5 * np.sum(dm * (h + F))) + e_nuc
             self.cycles = cycle + 1
-            if e_last is not None and abs(e - e_last) < self.conv_tol:
+            if final:
+                n_final += 1
+            de = abs(e - e_last) if e_last is not None else float('inf')
+            if de < self.conv_tol and final and (not mixed or n_final >= 2):
                 self.converged = True
                 break
+            if mixed and not final and de < self.mixed_switch_tol:
+                final = True
             e_last = e
             focks.append(F)
             errs.append((F @ dm @ S - S @ dm @ F).ravel())

@@ -153,6 +153,30 @@ int BQCbuild_jk_noalloc(const BasisProdCache *bpcache, const double *pair_q, dou
                         double *vk, const double *dm, int nao, int n_dm, double tol,
                         cudaStream_t stream);
 
+/* ---- learned initial density: BF16 tensor-core MLP kernels ----------------
+ * No reference counterpart (the reference starts from pyscf's minao guess).
+ * Row-major X (M x K, BF16), W (N x K, BF16); M, N, K multiples of 16
+ * (return 3 otherwise).  FP32 accumulation. */
+
+/* Z = X W^T + b (FP32, may be NULL); Yf / Yb = act(Z) in FP32 / BF16 (either
+ * may be NULL); act = ReLU when relu != 0, identity otherwise. */
+int BQCmlp_linear_fwd(const void *X, const void *W, const float *b, float *Z, float *Yf,
+                      void *Yb, int M, int N, int K, int relu, cudaStream_t stream);
+
+/* Backward of the layer: dZ = dY * (Z > 0) (Z == NULL: no activation), kept
+ * as BF16 in dZ_buf (M x N); dW = dZ^T X, db = sum_m dZ, dX = dZ W (dX may be
+ * NULL).  dW, db, dX are overwritten. */
+int BQCmlp_linear_bwd(const float *dY, const float *Z, const void *X, const void *W, void *dZ_buf,
+                      float *dX, float *dW, float *db, int M, int N, int K, cudaStream_t stream);
+
+/* Adam step on FP32 master weights w (n) with moments m, v; step counts from
+ * 1; refreshes the BF16 copy w_bf16 when not NULL. */
+int BQCmlp_adam(float *w, const float *g, float *m, float *v, void *w_bf16, int n, float lr,
+                float b1, float b2, float eps, int step, cudaStream_t stream);
+
+/* y = bf16(x), n elements. */
+int BQCmlp_to_bf16(const float *x, void *y, size_t n, cudaStream_t stream);
+
 /* Number of kernel launches the library has issued in this process. */
 unsigned long long BQClaunch_counter(void);
 

@@ -193,6 +193,12 @@ def test_mixed_precision_scf_energy(cuda):
     mf1.conv_tol = 1e-10
     mf1.fp32_threshold = 1e-6
     e1 = mf1.kernel()
-    assert mf0.converged and mf1.converged
+    mf2 = hf.RHF(mol)
+    mf2.conv_tol = 1e-10
+    mf2.fp32_threshold = 1e-6
+    mf2.early_tol = 1e-10
+    e2 = mf2.kernel()
+    assert mf0.converged and mf1.converged and mf2.converged
     assert abs(e1 - e0) < 1e-9
-    assert any(f > 0 for kind, f in mf1.build_log)
+    assert abs(e2 - e0) < 1e-9
+    assert any(rec[1] > 0 for rec in mf1.build_log)
