@@ -40,6 +40,7 @@ struct JKTask {
     // with tile_prefix[r] <= x < tile_prefix[r+1]; without it the grid is
     // the full rectangle.
     const int *tile_prefix;
+    const int *tile_col0;   // optional first column of each row (batched molecules)
     int nrows;
     int ntiles;        // number of tiles (blocks) when tile_prefix is set
     int rows_are_b;

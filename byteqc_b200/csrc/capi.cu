@@ -210,13 +210,53 @@ static int tile_rows(const double *qa, int na, const double *qb, int nb, double 
 
 // Launch (or, with count_dev, only count the surviving quartets of) every
 // class pair, or the single class pair (only_ij, only_kl) when only_ij >= 0.
+// Tile rows when the pairs of several independent molecules share the lists:
+// tiles hold pairs of one molecule, grouped by molecule in increasing order and
+// sorted by their first q within a molecule.  Row r may only meet the ket
+// tiles of its own molecule, [c0, c1); col0 receives c0 per row.
+static int tile_rows_mol(const double *qa, const int *ma, int na, const double *qb, const int *mb,
+                         int nb, double dm_max, double tol, int diag, std::vector<int> &prefix,
+                         std::vector<int> &col0) {
+    int nta = (na + 15) / 16, ntb = (nb + 15) / 16;
+    prefix.push_back(0);
+    int base = (int)prefix.size() - 1;
+    for (int r = 0; r < nta; r++) {
+        const int m = ma[16 * r];
+        int lo = 0, hi = ntb;   // first ket tile of molecule >= m
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            if (mb[16 * mid] < m) lo = mid + 1; else hi = mid;
+        }
+        const int c0 = lo;
+        hi = ntb;               // first ket tile of molecule > m
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            if (mb[16 * mid] <= m) lo = mid + 1; else hi = mid;
+        }
+        const int c1 = lo;
+        const double qr = qa[16 * r] * dm_max;
+        lo = c0;
+        hi = c1;
+        while (lo < hi) {
+            int mid = (lo + hi) / 2;
+            if (qb[16 * mid] * qr >= tol) lo = mid + 1; else hi = mid;
+        }
+        int n = lo - c0;
+        if (diag && n > r - c0 + 1) n = r - c0 + 1;
+        if (n < 0) n = 0;
+        prefix.push_back(prefix.back() + n);
+        col0.push_back(c0);
+    }
+    return prefix.back() - prefix[base];
+}
+
 static int build_jk_band(const BasisProdCache *bp, JKArgs args, const double *pair_q_host,
-                         double dm_max, int fp32, int only_ij, int only_kl,
-                         unsigned long long *count_dev, cudaStream_t stream) {
+                         const int *pair_mol_host, double dm_max, int fp32, int only_ij,
+                         int only_kl, unsigned long long *count_dev, cudaStream_t stream) {
     std::vector<JKTask> tasks;
     std::vector<int> shape;   // (li, lj, lk, ll) per task
-    std::vector<int> prefix;
-    std::vector<size_t> prefix_off;
+    std::vector<int> prefix, col0;
+    std::vector<size_t> prefix_off, col0_off;
     for (int cij = 0; cij < bp->ncptype; cij++) {
         const ContractionProdType *tij = bp->cptype + cij;
         if (tij->npairs == 0) continue;
@@ -239,16 +279,24 @@ static int build_jk_band(const BasisProdCache *bp, JKArgs args, const double *pa
             t.diag = cij == ckl;
             t.skip_lower = 1;
             if (pair_q_host != nullptr) {
-                size_t off = prefix.size();
-                int n = tile_rows(pair_q_host + t.a0, t.na, pair_q_host + t.b0, t.nb, dm_max,
+                size_t off = prefix.size(), coff = col0.size();
+                int n;
+                if (pair_mol_host != nullptr)
+                    n = tile_rows_mol(pair_q_host + t.a0, pair_mol_host + t.a0, t.na,
+                                      pair_q_host + t.b0, pair_mol_host + t.b0, t.nb, dm_max,
+                                      args.tol, t.diag, prefix, col0);
+                else
+                    n = tile_rows(pair_q_host + t.a0, t.na, pair_q_host + t.b0, t.nb, dm_max,
                                   args.tol, t.diag, prefix);
                 if (n == 0) {
                     prefix.resize(off);
+                    col0.resize(coff);
                     continue;
                 }
                 t.nrows = (t.na + 15) / 16;
                 t.ntiles = n;
                 prefix_off.push_back(off);
+                col0_off.push_back(coff);
             }
             tasks.push_back(t);
             shape.push_back(tij->l_bra);
@@ -259,14 +307,18 @@ static int build_jk_band(const BasisProdCache *bp, JKArgs args, const double *pa
     }
     int *d_prefix = nullptr;
     if (pair_q_host != nullptr && !prefix.empty()) {
-        if (cudaMallocAsync((void **)&d_prefix, sizeof(int) * prefix.size(), stream) != cudaSuccess)
+        const size_t n_all = prefix.size() + col0.size();
+        if (cudaMallocAsync((void **)&d_prefix, sizeof(int) * n_all, stream) != cudaSuccess)
             return 1;
-        cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int) * prefix.size(),
-                        cudaMemcpyHostToDevice, stream);
+        prefix.insert(prefix.end(), col0.begin(), col0.end());
+        cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(int) * n_all, cudaMemcpyHostToDevice,
+                        stream);
     }
+    const size_t col0_base = prefix.size() - col0.size();
     int err = 0;
     for (size_t i = 0; i < tasks.size() && !err; i++) {
         if (d_prefix) tasks[i].tile_prefix = d_prefix + prefix_off[i];
+        if (d_prefix && pair_mol_host != nullptr) tasks[i].tile_col0 = d_prefix + col0_base + col0_off[i];
         if (count_dev != nullptr)
             err = bqc_launch_count(args, tasks[i], count_dev, stream);
         else
@@ -282,7 +334,8 @@ static int build_jk_band(const BasisProdCache *bp, JKArgs args, const double *pa
 // With fp32_below > tol the quartets split into two bands: bound >= fp32_below
 // in FP64 and tol <= bound < fp32_below in FP32 (count_dev counts both).
 static int build_jk_impl(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
-                         const double *dm_cond, double dm_max, double *vj, double *vk,
+                         const int *pair_mol_host, const double *dm_cond, double dm_max,
+                         double *vj, double *vk,
                          const double *dm, int nao, int n_dm, double tol, double fp32_below,
                          int *status_dev, int only_ij, int only_kl,
                          unsigned long long *count_dev, cudaStream_t stream) {
@@ -294,22 +347,34 @@ static int build_jk_impl(const BasisProdCache *bp, const double *pair_q, const d
     args.status = status_dev;
     if (dm_cond == nullptr) dm_max = 1.0;
     if (pair_q == nullptr || fp32_below <= tol)
-        return build_jk_band(bp, args, pair_q_host, dm_max, 0, only_ij, only_kl, count_dev, stream);
+        return build_jk_band(bp, args, pair_q_host, pair_mol_host, dm_max, 0, only_ij, only_kl,
+                             count_dev, stream);
     JKArgs hi = args;
     hi.tol = fp32_below;
-    int err = build_jk_band(bp, hi, pair_q_host, dm_max, 0, only_ij, only_kl, count_dev, stream);
+    int err = build_jk_band(bp, hi, pair_q_host, pair_mol_host, dm_max, 0, only_ij, only_kl,
+                            count_dev, stream);
     if (err) return err;
     JKArgs lo = args;
     lo.tol_hi = fp32_below;
-    return build_jk_band(bp, lo, pair_q_host, dm_max, 1, only_ij, only_kl, count_dev, stream);
+    return build_jk_band(bp, lo, pair_q_host, pair_mol_host, dm_max, 1, only_ij, only_kl,
+                         count_dev, stream);
 }
 
 int BQCbuild_jk(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
                 const double *dm_cond, double dm_max, double *vj, double *vk, const double *dm,
                 int nao, int n_dm, double tol, double fp32_below, int *status_dev,
                 cudaStream_t stream) {
-    return build_jk_impl(bp, pair_q, pair_q_host, dm_cond, dm_max, vj, vk, dm, nao, n_dm, tol,
+    return build_jk_impl(bp, pair_q, pair_q_host, nullptr, dm_cond, dm_max, vj, vk, dm, nao, n_dm, tol,
                          fp32_below, status_dev, -1, -1, nullptr, stream);
+}
+
+int BQCbuild_jk_mol(const BasisProdCache *bp, const double *pair_q, const double *pair_q_host,
+                    const int *pair_mol_host, const double *dm_cond, double dm_max, double *vj,
+                    double *vk, const double *dm, int nao, int n_dm, double tol, double fp32_below,
+                    int *status_dev, cudaStream_t stream) {
+    if (pair_q_host == nullptr || pair_mol_host == nullptr) return 1;
+    return build_jk_impl(bp, pair_q, pair_q_host, pair_mol_host, dm_cond, dm_max, vj, vk, dm, nao,
+                         n_dm, tol, fp32_below, status_dev, -1, -1, nullptr, stream);
 }
 
 int BQCbuild_jk_class(const BasisProdCache *bp, int cp_ij, int cp_kl, const double *pair_q,
@@ -317,7 +382,7 @@ int BQCbuild_jk_class(const BasisProdCache *bp, int cp_ij, int cp_kl, const doub
                       double *vk, const double *dm, int nao, int n_dm, double tol,
                       double fp32_below, int *status_dev, cudaStream_t stream) {
     if (cp_ij < 0 || cp_kl < 0 || cp_kl > cp_ij || cp_ij >= bp->ncptype) return 1;
-    return build_jk_impl(bp, pair_q, pair_q_host, dm_cond, dm_max, vj, vk, dm, nao, n_dm, tol,
+    return build_jk_impl(bp, pair_q, pair_q_host, nullptr, dm_cond, dm_max, vj, vk, dm, nao, n_dm, tol,
                          fp32_below, status_dev, cp_ij, cp_kl, nullptr, stream);
 }
 
@@ -325,7 +390,7 @@ int BQCcount_quartets(const BasisProdCache *bp, int cp_ij, int cp_kl, const doub
                       const double *pair_q_host, const double *dm_cond, double dm_max, double tol,
                       unsigned long long *count_dev, cudaStream_t stream) {
     if (count_dev == nullptr) return 1;
-    return build_jk_impl(bp, pair_q, pair_q_host, dm_cond, dm_max, nullptr, nullptr, nullptr, 0, 0,
+    return build_jk_impl(bp, pair_q, pair_q_host, nullptr, dm_cond, dm_max, nullptr, nullptr, nullptr, 0, 0,
                          tol, 0., nullptr, cp_ij, cp_kl, count_dev, stream);
 }
 
@@ -388,7 +453,7 @@ int BQCbuild_jk_noalloc(const BasisProdCache *bp, const double *pair_q, double *
     // every entry of the nbas x nbas table is overwritten before it is read
     int err = bqc_launch_dm_cond(dm, n_dm, nao, bp->ao_loc, bp->nbas, dm_cond, stream);
     if (err) return err;
-    return build_jk_impl(bp, pair_q, nullptr, dm_cond, 1.0, vj, vk, dm, nao, n_dm, tol, 0.,
+    return build_jk_impl(bp, pair_q, nullptr, nullptr, dm_cond, 1.0, vj, vk, dm, nao, n_dm, tol, 0.,
                          nullptr, -1, -1, nullptr, stream);
 }
 

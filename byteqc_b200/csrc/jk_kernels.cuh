@@ -56,6 +56,7 @@ __device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, in
         }
         r = lo;
         c = x - __ldg(T.tile_prefix + r);
+        if (T.tile_col0 != nullptr) c += __ldg(T.tile_col0 + r);
     } else {
         int ncols = ((T.rows_are_b ? T.na : T.nb) + TILE - 1) / TILE;
         r = blockIdx.x / ncols;
@@ -378,6 +379,7 @@ __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
         }
         r = lo;
         c = x - __ldg(T.tile_prefix + r);
+        if (T.tile_col0 != nullptr) c += __ldg(T.tile_col0 + r);
     } else {
         int ncols = ((T.rows_are_b ? T.na : T.nb) + TILE - 1) / TILE;
         r = blockIdx.x / ncols;

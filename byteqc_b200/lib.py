@@ -15,7 +15,7 @@ _lib = None
 
 # exported symbols, as declared in include/byteqc_b200.h
 SYMBOLS = ('GINTinit_basis_prod_cpu', 'GINTinit_basis_prod_gpu', 'GINTdel_basis_prod',
-           'GINTbuild_jk', 'BQCbuild_jk', 'BQCbuild_jk_class', 'BQCcount_quartets',
+           'GINTbuild_jk', 'BQCbuild_jk', 'BQCbuild_jk_mol', 'BQCbuild_jk_class', 'BQCcount_quartets',
            'BQCfp64_fma_peak', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e', 'BQClaunch_counter',
            'BQCbuild_jk_noalloc', 'BQCmlp_linear_fwd', 'BQCmlp_linear_bwd', 'BQCmlp_adam',
            'BQCmlp_to_bf16', 'BQCversion')
@@ -46,6 +46,10 @@ def load_library(name='libbyteqc_b200'):
         [ctypes.c_void_p] * 3 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                                  ctypes.c_void_p]
     lib.BQCbuild_jk_noalloc.restype = ctypes.c_int
+    lib.BQCbuild_jk_mol.restype = ctypes.c_int
+    lib.BQCbuild_jk_mol.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_double] + \
+        [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_void_p, ctypes.c_void_p]
     vp, ci, cf = ctypes.c_void_p, ctypes.c_int, ctypes.c_float
     lib.BQCmlp_linear_fwd.argtypes = [vp] * 6 + [ci] * 4 + [vp]
     lib.BQCmlp_linear_bwd.argtypes = [vp] * 8 + [ci] * 3 + [vp]

@@ -1,0 +1,349 @@
+"""Batched restricted HF: many independent molecules solved together.
+
+All molecules share one set of pair lists (shells ordered molecule by
+molecule; within each (l, nprim) x (l, nprim) class the 16-pair tiles are
+grouped by molecule and sorted by their largest Schwarz factor), so one
+``BQCbuild_jk_mol`` call builds J and K of every molecule with one launch per
+class pair; quartets never mix molecules.  The AO densities and J/K live in
+one block-diagonal matrix over all molecules (HBM holds it easily: 51k
+Cartesian AOs for 256 (H2O)_k, k <= 12); the SCF linear algebra (DIIS,
+generalized eigenproblem, density, energy) runs batched over a padded stack.
+"""
+import ctypes
+import time
+
+import numpy as np
+import torch
+
+from .. import lib as _libmod
+from ..gto import mole as gto
+from .hf import _VHFOpt, _dev, _ptr, _stream, basis_seg_contraction, _tile_order, PAIR_TILE
+from .guess import atomic_density
+
+
+class BatchedVHFOpt:
+    """Combined decontracted basis of many molecules with intra-molecular
+    pair lists."""
+
+    def __init__(self, mols, cutoff=1e-13):
+        self.mols = mols
+        self.direct_scf_tol = cutoff
+        parts = [basis_seg_contraction(m) for m in mols]
+        self.coeffs = [c for _, c in parts]
+        # concatenate the Cartesian molecules (pointer offsets into one env)
+        atm, bas, env = [], [], [np.zeros(gto.PTR_ENV_START)]
+        shell_mol = []
+        natm = 0
+        off = gto.PTR_ENV_START
+        for m, (pmol, _) in enumerate(parts):
+            e = pmol._env[gto.PTR_ENV_START:]
+            a = pmol._atm.copy()
+            a[:, gto.PTR_COORD] += off - gto.PTR_ENV_START
+            a[:, 3] += off - gto.PTR_ENV_START
+            b = pmol._bas.copy()
+            b[:, gto.ATOM_OF] += natm
+            b[:, gto.PTR_EXP] += off - gto.PTR_ENV_START
+            b[:, gto.PTR_COEFF] += off - gto.PTR_ENV_START
+            # (l, nprim) sort inside the molecule keeps classes uniform
+            order = np.lexsort((b[:, gto.NPRIM_OF], b[:, gto.ANG_OF]))
+            self.coeffs[m] = self._sort_coeff(pmol, order, self.coeffs[m])
+            b = b[order]
+            atm.append(a)
+            bas.append(b)
+            env.append(e)
+            shell_mol += [m] * len(b)
+            natm += len(a)
+            off += len(e)
+        big = mols[0].copy()
+        big._atm = np.vstack(atm).astype(np.int32)
+        big._bas = np.vstack(bas).astype(np.int32)
+        big._env = np.concatenate(env)
+        big.cart = True
+        self.mol = big
+        self.shell_mol = np.asarray(shell_mol, dtype=np.int32)
+        ao_loc = big.ao_loc_nr(cart=True)
+        self.ao_off = np.array([ao_loc[np.flatnonzero(self.shell_mol == m)[0]] for m in range(len(mols))]
+                               + [ao_loc[-1]])
+        self.nao_cart = int(ao_loc[-1])
+
+    @staticmethod
+    def _sort_coeff(pmol, order, coeff):
+        ao_loc = pmol.ao_loc_nr(cart=True)
+        idx = np.hstack([np.arange(ao_loc[i], ao_loc[i + 1]) for i in order])
+        return coeff[idx]
+
+    def build(self):
+        lib = _libmod.load_library()
+        mol = self.mol
+        key = mol._bas[:, gto.ANG_OF] * 1000 + mol._bas[:, gto.NPRIM_OF]
+        groups = np.unique(key)
+        gid = np.searchsorted(groups, key)
+        shells_of = [np.flatnonzero(gid == g) for g in range(len(groups))]
+        pair_lists = []
+        for p in range(len(groups)):
+            for q in range(p + 1):
+                i = np.repeat(shells_of[p], len(shells_of[q]))
+                j = np.tile(shells_of[q], len(shells_of[p]))
+                m = self.shell_mol[i] == self.shell_mol[j]
+                if p == q:
+                    m &= i >= j
+                pair_lists.append((i[m], j[m]))
+        ncp = len(pair_lists)
+        locs = np.append(0, np.cumsum([len(x[0]) for x in pair_lists])).astype(np.int32)
+        p2s = np.vstack([np.hstack([x[0] for x in pair_lists]),
+                         np.hstack([x[1] for x in pair_lists])]).astype(np.int32)
+        helper = _VHFOpt.__new__(_VHFOpt)
+        helper.mol = mol
+        bp_cpu, bp_gpu, mem, keep = helper._init_cache(p2s, locs, ncp, 0.5)
+        q_all = torch.zeros(max(int(locs[-1]), 1), dtype=torch.float64, device=_dev())
+        for c in range(ncp):
+            if locs[c + 1] > locs[c]:
+                err = lib.BQCschwarz(bp_gpu, ctypes.c_int(c), ctypes.c_double(0.5),
+                                     _ptr(q_all[locs[c]:]), _stream())
+                if err:
+                    raise RuntimeError('BQCschwarz failed (%d)' % err)
+        q_all = q_all.cpu().numpy()
+        helper._free_cache(bp_cpu, bp_gpu)
+        del mem, keep
+        b_all, k_all, q_out, mol_out, dummies, new_locs = [], [], [], [], [], [0]
+        for c in range(ncp):
+            sl = slice(locs[c], locs[c + 1])
+            b, k, q = p2s[0, sl], p2s[1, sl], q_all[sl]
+            keepm = q > self.direct_scf_tol
+            b, k, q = b[keepm], k[keepm], q[keepm]
+            mb = self.shell_mol[b]
+            for m in np.unique(mb):
+                s = mb == m
+                tb, tk, tq, td = _tile_order(b[s], k[s], q[s])
+                b_all.append(tb)
+                k_all.append(tk)
+                q_out.append(tq)
+                dummies.append(td)
+                mol_out.append(np.full(len(tb), m, dtype=np.int32))
+            new_locs.append(new_locs[-1] + sum(len(x) for x in b_all[len(mol_out) - len(np.unique(mb)):]))
+        self.bas_pairs_locs = np.asarray(new_locs, dtype=np.int32)
+        cat = lambda x, dt: np.hstack(x).astype(dt) if x else np.zeros(0, dt)
+        self.bas_pair2shls = np.vstack([cat(b_all, np.int32), cat(k_all, np.int32)])
+        self.pair_dummy = cat(dummies, bool)
+        self.pair_mol_host = np.ascontiguousarray(cat(mol_out, np.int32))
+        self.pair_q_host = np.ascontiguousarray(cat(q_out, np.float64))
+        self.ncptype = ncp
+        self._helper = helper
+        self._bp_cpu, self._bp_gpu, self._mem, self._keep = helper._init_cache(
+            self.bas_pair2shls, self.bas_pairs_locs, ncp, 0.5, self.pair_dummy)
+        self.pair_q = torch.as_tensor(self.pair_q_host, device=_dev())
+        return self
+
+    def jk_cart(self, dmc, tol=None, fp32_below=0.):
+        """J', K' of the block-diagonal Cartesian density dmc (1, n, n)."""
+        lib = _libmod.load_library()
+        n = dmc.shape[-1]
+        nbas = self.mol.nbas
+        dm_cond = torch.empty((nbas, nbas), dtype=torch.float64, device=dmc.device)
+        err = lib.BQCdm_cond(_ptr(dmc), ctypes.c_int(1), ctypes.c_int(n), _ptr(self._mem['ao_loc']),
+                             ctypes.c_int(nbas), _ptr(dm_cond), _stream())
+        if err:
+            raise RuntimeError('BQCdm_cond failed (%d)' % err)
+        vj = torch.zeros_like(dmc)
+        vk = torch.zeros_like(dmc)
+        err = lib.BQCbuild_jk_mol(ctypes.cast(self._bp_gpu, ctypes.c_void_p), _ptr(self.pair_q),
+                                  self.pair_q_host.ctypes.data_as(ctypes.c_void_p),
+                                  self.pair_mol_host.ctypes.data_as(ctypes.c_void_p),
+                                  _ptr(dm_cond), float(dm_cond.max()), _ptr(vj), _ptr(vk),
+                                  _ptr(dmc), n, 1, self.direct_scf_tol if tol is None else tol,
+                                  fp32_below, None, _stream())
+        if err:
+            raise RuntimeError('BQCbuild_jk_mol failed (%d)' % err)
+        return vj, vk
+
+
+class BatchedRHF:
+    """RHF of many molecules in lock step: one batched J/K build per cycle,
+    padded batched DIIS / eigensolver; SAD guess; incremental Fock builds.
+    Converged molecules keep their Fock matrix (their density no longer
+    changes, so the difference density screens their quartets out)."""
+
+    def __init__(self, mols):
+        self.mols = mols
+        self.conv_tol = 1e-9
+        self.max_cycle = 60
+        self.diis_space = 8
+        self.timings = {}
+
+    def kernel(self):
+        t0 = time.perf_counter()
+        dev = _dev()
+        mols = self.mols
+        B = len(mols)
+        opt = self.opt = BatchedVHFOpt(mols).build()
+        n0 = np.array([m.nao for m in mols])
+        nmax = int(n0.max())
+        nc = np.diff(opt.ao_off)
+        ncmax = int(nc.max())
+        # padded per-molecule matrices
+        S = torch.zeros((B, nmax, nmax), dtype=torch.float64, device=dev)
+        H = torch.zeros_like(S)
+        C = torch.zeros((B, ncmax, nmax), dtype=torch.float64, device=dev)
+        D = torch.zeros_like(S)
+        e_nuc = torch.tensor([m.energy_nuc() for m in mols], dtype=torch.float64, device=dev)
+        for b, m in enumerate(mols):
+            single = _VHFOpt.__new__(_VHFOpt)
+            single.mol, single.coeff = basis_seg_contraction(m)
+            single.coeff_dev = torch.as_tensor(single.coeff, device=dev)
+            single.nao_cart = single.coeff.shape[0]
+            single._mem = {'ao_loc': torch.as_tensor(single.mol.ao_loc_nr(cart=True),
+                                                     dtype=torch.int32, device=dev)}
+            s, t, v = single.int1e()
+            S[b, :n0[b], :n0[b]] = s
+            H[b, :n0[b], :n0[b]] = t + v
+            C[b, :nc[b], :n0[b]] = torch.as_tensor(opt.coeffs[b], device=dev)
+            sl = m.aoslice_by_atom()
+            for ia, (sym, _) in enumerate(m.atom):
+                D[b, sl[ia, 2]:sl[ia, 3], sl[ia, 2]:sl[ia, 3]] = atomic_density(sym, m.basis)
+            ne = float(torch.sum(D[b] * S[b]))
+            D[b] *= m.nelectron / ne
+        # canonical orthogonalisation, padded rows/columns stay zero
+        pad = torch.zeros((B, nmax), dtype=torch.bool, device=dev)
+        for b in range(B):
+            pad[b, n0[b]:] = True
+        X = torch.zeros_like(S)
+        for b in range(B):
+            w, U = torch.linalg.eigh(S[b, :n0[b], :n0[b]])
+            X[b, :n0[b], :n0[b]] = U * torch.where(w > 1e-12, 1. / torch.sqrt(w.clamp_min(1e-300)), 0.)
+        nocc = torch.tensor([m.nelectron // 2 for m in mols], device=dev)
+        # gather indices of the diagonal blocks of the block-diagonal matrix
+        rows, cols, bid, ri, ci = [], [], [], [], []
+        for b in range(B):
+            o, n = opt.ao_off[b], nc[b]
+            r, c = np.meshgrid(np.arange(n), np.arange(n), indexing='ij')
+            rows.append(o + r.ravel()); cols.append(o + c.ravel())
+            bid.append(np.full(n * n, b)); ri.append(r.ravel()); ci.append(c.ravel())
+        cat = lambda x: torch.as_tensor(np.concatenate(x), device=dev)
+        rows, cols, bid, ri, ci = cat(rows), cat(cols), cat(bid), cat(ri), cat(ci)
+        N = opt.nao_cart
+        torch.cuda.synchronize()
+        self.timings['setup'] = time.perf_counter() - t0
+
+        def jk(dmat):
+            dcp = C @ dmat @ C.transpose(1, 2)                      # (B, ncmax, ncmax)
+            big = torch.zeros((1, N, N), dtype=torch.float64, device=dev)
+            big[0, rows, cols] = dcp[bid, ri, ci]
+            vj, vk = opt.jk_cart(big)
+            J = torch.zeros_like(dcp)
+            K = torch.zeros_like(dcp)
+            J[bid, ri, ci] = vj[0, rows, cols]
+            K[bid, ri, ci] = vk[0, rows, cols]
+            J = 2 * (J + J.transpose(1, 2))
+            K = K + K.transpose(1, 2)
+            Ct = C.transpose(1, 2)
+            return Ct @ J @ C, Ct @ K @ C
+
+        vj, vk = jk(D)
+        e_last = None
+        done = torch.zeros(B, dtype=torch.bool, device=dev)
+        focks, errs = [], []
+        # orthogonal directions that do not exist (padding, dropped linear
+        # dependencies) get a huge orbital energy so they are never occupied
+        big_diag = 1e6 * torch.diag_embed((X.abs().sum(1) == 0).double())
+        t_jk = 0.
+        for cycle in range(self.max_cycle):
+            F = H + vj - .5 * vk
+            e = .5 * torch.einsum('bij,bij->b', D, H + F) + e_nuc
+            if e_last is not None:
+                done = done | ((e - e_last).abs() < self.conv_tol)
+                if bool(done.all()):
+                    break
+            e_last = e
+            err = X.transpose(1, 2) @ (F @ D @ S - S @ D @ F) @ X
+            focks.append(F); errs.append(err)
+            focks, errs = focks[-self.diis_space:], errs[-self.diis_space:]
+            k = len(focks)
+            if k > 1:
+                E = torch.stack(errs, 1).reshape(B, k, -1)
+                Bm = torch.zeros((B, k + 1, k + 1), dtype=torch.float64, device=dev)
+                G = E @ E.transpose(1, 2)
+                scale = torch.diagonal(G, dim1=1, dim2=2).amax(1).clamp_min(1e-300)
+                Bm[:, :k, :k] = G + (1e-14 * scale)[:, None, None] * torch.eye(k, device=dev,
+                                                                              dtype=torch.float64)
+                Bm[:, k, :k] = -1
+                Bm[:, :k, k] = -1
+                rhs = torch.zeros((B, k + 1), dtype=torch.float64, device=dev)
+                rhs[:, k] = -1
+                cvec = torch.linalg.solve(Bm, rhs)[:, :k]
+                Fd = torch.einsum('bk,kbij->bij', cvec, torch.stack(focks))
+            else:
+                Fd = F
+            Fo = X.transpose(1, 2) @ Fd @ X + big_diag
+            mo_e, mo_c = torch.linalg.eigh(Fo)
+            mo_c = X @ mo_c
+            occ = (torch.arange(nmax, device=dev)[None, :] < nocc[:, None]).double()
+            Dn = 2 * (mo_c * occ[:, None, :]) @ mo_c.transpose(1, 2)
+            Dn = torch.where(done[:, None, None], D, Dn)
+            tj = time.perf_counter()
+            dvj, dvk = jk(Dn - D)
+            torch.cuda.synchronize()
+            t_jk += time.perf_counter() - tj
+            vj, vk = vj + dvj, vk + dvk
+            D = Dn
+        self.cycles = cycle + 1
+        self.converged = bool(done.all())
+        self.e_tot = e.cpu().numpy()
+        self.timings['jk'] = t_jk
+        self.timings['total'] = time.perf_counter() - t0
+        return self.e_tot
+
+
+def batch_systems(nmol, kmin=1, kmax=12, seed=0):
+    """Seeded (H2O)_k, k uniform in [kmin, kmax], cc-pVDZ-shaped basis."""
+    from ..gto.basis import synthetic_basis
+    from ..gto.geom import water_cluster
+    rng = np.random.default_rng(seed)
+    basis = synthetic_basis('cc-pvdz', ['O', 'H'])
+    ks = rng.integers(kmin, kmax + 1, nmol)
+    return [gto.Mole(water_cluster(int(k), seed=int(seed * 100000 + i)), basis)
+            for i, k in enumerate(ks)]
+
+
+def main(argv=None):
+    """Molecules/s of one batched solve against one-by-one plain solves.
+
+        python -m byteqc_b200.scf.batched --nmol 256 [--seq 256]
+    """
+    import argparse
+    import json
+    from . import hf
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--nmol', type=int, default=256)
+    ap.add_argument('--seq', type=int, default=None, help='sequential solves to time (default all)')
+    ap.add_argument('--conv', type=float, default=1e-9)
+    a = ap.parse_args(argv)
+    mols = batch_systems(a.nmol)
+    BatchedRHF(mols[:2]).kernel()          # warm-up (library load, SAD atoms)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mf = BatchedRHF(mols)
+    mf.conv_tol = a.conv
+    e = mf.kernel()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    nseq = a.nmol if a.seq is None else a.seq
+    t0 = time.perf_counter()
+    es = []
+    for m in mols[:nseq]:
+        one = hf.RHF(m)
+        one.conv_tol = a.conv
+        es.append(one.kernel())
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    out = {'nmol': a.nmol, 'nao_total': int(sum(m.nao for m in mols)),
+           'batched_s': t_batch, 'batched_mol_per_s': a.nmol / t_batch,
+           'batched_cycles': mf.cycles, 'batched_converged': mf.converged,
+           'batched_timings': mf.timings,
+           'sequential_n': nseq, 'sequential_s': t_seq, 'sequential_mol_per_s': nseq / t_seq,
+           'speedup': (a.nmol / t_batch) / (nseq / t_seq),
+           'max_energy_diff': float(np.max(np.abs(np.asarray(es) - e[:nseq])))}
+    print(json.dumps(out))
+
+
+if __name__ == '__main__':
+    main()

@@ -103,6 +103,18 @@ int BQCbuild_jk(const BasisProdCache *bpcache, const double *pair_q, const doubl
                 int nao, int n_dm, double tol, double fp32_below, int *status_dev,
                 cudaStream_t stream);
 
+/* BQCbuild_jk over the pair lists of many independent molecules at once (no
+ * reference counterpart; the batched form).  pair_mol_host gives the
+ * molecule of every pair; within each class the 16-pair tiles hold pairs of
+ * one molecule, are grouped by molecule in increasing order and sorted by
+ * their first q within a molecule.  Only quartets within one molecule are
+ * formed; one launch per class pair covers every molecule.  dm/vj/vk are the
+ * block-diagonal matrices of all molecules (nao = total AO count). */
+int BQCbuild_jk_mol(const BasisProdCache *bpcache, const double *pair_q, const double *pair_q_host,
+                    const int *pair_mol_host, const double *dm_cond, double dm_max, double *vj,
+                    double *vk, const double *dm, int nao, int n_dm, double tol, double fp32_below,
+                    int *status_dev, cudaStream_t stream);
+
 /* One class pair (cp_ij >= cp_kl) of BQCbuild_jk, same arguments otherwise;
  * lets a caller time or profile the kernels class by class. */
 int BQCbuild_jk_class(const BasisProdCache *bpcache, int cp_ij, int cp_kl, const double *pair_q,
