@@ -322,9 +322,10 @@ __global__ void __launch_bounds__(256) jk_small(JKArgs A, JKTask T) {
 // Contributions that share a target are summed across the tile before the
 // atomics: J_ij over the 16 kets of a row, J_kl over the 16 bras of a
 // column (warp shuffles, then shared memory across the 8 warps); when all
-// bra pairs of the tile share the bra shell i (the pair lists are laid out
-// that way, see _tile_order) K_il is summed over a column, when all ket
-// pairs share k, K_jk over a row, and K_ik over both.
+// bra pairs of the tile share the bra shell i (the 'shell' pair layout of
+// _tile_order guarantees it) K_il is summed over a column, when all ket
+// pairs share k, K_jk over a row, and K_ik over both; otherwise these K
+// targets take one atomic per quartet.
 template <int NV>
 __device__ __forceinline__ void row_reduce(double (&v)[NV]) {
 #pragma unroll

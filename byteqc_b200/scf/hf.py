@@ -109,15 +109,58 @@ def _make_s_index_offsets(log_q, nbins=10, cutoff=1e-12):
 PAIR_TILE = 16
 
 
-def _tile_order(bra, ket, q):
-    """Order the pairs of one class in tiles of PAIR_TILE pairs that share the
-    bra shell: pairs are grouped by bra shell, sorted by q descending within a
-    group, cut into tiles (the last tile of a group padded with pairs of
-    q = 0), and the tiles are sorted by their largest q.  So q is descending
-    within a tile and the first q of every tile is descending along the list,
-    which keeps the tile pruning of BQCbuild_jk valid, and a J/K kernel can
-    reduce the contributions that share a shell across a tile.  Returns
-    (bra, ket, q, is_padding)."""
+def _tile_order(bra, ket, q, layout='q'):
+    """Order the pairs of one class in tiles of PAIR_TILE pairs.
+
+    layout 'q': all pairs sorted by q descending, the last tile padded with
+    pairs of q = 0.  Every tile spans a narrow range of q, so almost every
+    quartet of a launched tile pair passes the device screen.
+    layout 'shell': tiles of pairs that share the bra shell: pairs grouped by
+    bra shell, sorted by q descending within a group, cut into tiles (the
+    last tile of a group padded), tiles sorted by their largest q.  A J/K
+    kernel can then sum the K contributions that share a shell across the
+    tile before its atomics, but small groups leave tiles mostly padding.
+
+    layout 'hybrid': the full tiles of the 'shell' layout (bra-shell groups
+    of at least PAIR_TILE pairs), all remaining pairs packed in the 'q'
+    layout, tiles sorted by their largest q.
+
+    In every layout q is descending within a tile and the first q of every
+    tile is descending along the list, which keeps the tile pruning of
+    BQCbuild_jk valid.  Returns (bra, ket, q, is_padding)."""
+    if layout == 'hybrid':
+        n = len(q)
+        if n == 0:
+            return bra, ket, q, np.zeros(0, bool)
+        o = np.lexsort((-q, bra))
+        b, k, qq = bra[o], ket[o], q[o]
+        starts = np.flatnonzero(np.r_[True, b[1:] != b[:-1]])
+        sizes = np.diff(np.r_[starts, n])
+        gid = np.repeat(np.arange(len(starts)), sizes)
+        rank = np.arange(n) - starts[gid]
+        full = rank < (sizes[gid] // PAIR_TILE) * PAIR_TILE
+        rest = np.flatnonzero(~full)
+        rest = rest[np.argsort(-qq[rest], kind='stable')]
+        pad = (-len(rest)) % PAIR_TILE
+        idx = np.r_[np.flatnonzero(full), rest, np.full(pad, rest[-1] if len(rest) else 0)]
+        tb, tk = b[idx].reshape(-1, PAIR_TILE), k[idx].reshape(-1, PAIR_TILE)
+        tq = np.r_[qq[idx[:n]], np.zeros(pad)].reshape(-1, PAIR_TILE)
+        ot = np.argsort(-tq[:, 0], kind='stable')
+        dummy = np.r_[np.zeros(n, bool), np.ones(pad, bool)].reshape(-1, PAIR_TILE)[ot]
+        return tb[ot].ravel(), tk[ot].ravel(), tq[ot].ravel(), dummy.ravel()
+    if layout == 'q':
+        n = len(q)
+        o = np.argsort(-q, kind='stable')
+        pad = (-n) % PAIR_TILE
+        if n == 0:
+            return bra, ket, q, np.zeros(0, bool)
+        out_b = np.r_[bra[o], np.repeat(bra[o[-1:]], pad)]
+        out_k = np.r_[ket[o], np.repeat(ket[o[-1:]], pad)]
+        out_q = np.r_[q[o], np.zeros(pad)]
+        dummy = np.r_[np.zeros(n, bool), np.ones(pad, bool)]
+        return out_b, out_k, out_q, dummy
+    if layout != 'shell':
+        raise ValueError('unknown tile layout %r' % layout)
     n = len(q)
     if n == 0:
         return bra, ket, q, np.zeros(0, bool)
@@ -169,6 +212,8 @@ class _VHFOpt:
         self.mol, self.coeff = basis_seg_contraction(mol)
         self._intor = intor
         self.direct_scf_tol = 1e-13
+        # pair layout of the tiles (see _tile_order)
+        self.tile_layout = 'hybrid'
         self._bp_cpu = None
         self._bp_gpu = None
 
@@ -275,13 +320,13 @@ class _VHFOpt:
         del mem, keep
 
         # pass 2: keep q > cutoff and lay every class out in tiles of 16 pairs
-        # sharing the bra shell (see _tile_order)
+        # (see _tile_order)
         pair2bra, pair2ket, qs, log_qs, dummies = [], [], [], [], []
         for c in range(ncptype):
             q = q_all[locs[c]:locs[c + 1]]
             keep = q > cutoff
             b, k, q = p2s[0, locs[c]:locs[c + 1]][keep], p2s[1, locs[c]:locs[c + 1]][keep], q[keep]
-            b, k, q, dummy = _tile_order(b, k, q)
+            b, k, q, dummy = _tile_order(b, k, q, self.tile_layout)
             pair2bra.append(b)
             pair2ket.append(k)
             qs.append(q)

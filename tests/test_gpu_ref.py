@@ -5,7 +5,9 @@ The reference libraries are driven through the same C ABI as this package's:
 its GINTinit_basis_prod_cpu/_gpu build its own basis-product cache from the
 engine's pair lists (padding pairs removed), and its GINTbuild_jk runs every
 class pair with one bin (no density screening).  J and K must agree with the
-CPU oracle and with this engine to 1e-10.
+CPU oracle and with this engine to 1e-10.  With the reference's own host
+screening (oracle/ref_gpu.py: log q bins, class-level density bound) the two
+builds differ only by what each screen drops.
 """
 import ctypes
 import os
@@ -108,3 +110,29 @@ def test_reference_kernels_agree(cuda, kind):
     # as cuobc/scf/hf.py does, release through the device copy only (it owns
     # the class table and pair block it shares with the host cache)
     lg.GINTdel_basis_prod(ctypes.byref(bpg))
+
+
+def test_reference_screened_build_agrees(cuda):
+    import torch
+    from byteqc_b200.scf import hf
+    from oracle import ref_gpu
+    if not ref_gpu.available():
+        pytest.skip('reference libraries not built (oracle/build_ref.sh)')
+    mol = Mole(water_cluster(3, seed=2), synthetic_basis('cc-pvdz', ['O', 'H']))
+    mf = hf.RHF(mol)
+    mf.kernel()
+    opt = mf.opt
+    ref = ref_gpu.RefJK(opt)
+    C = opt.coeff_dev
+    dmc = (C @ mf.dm @ C.T)[None].contiguous()
+    J1, K1 = opt.jk_cart(dmc)
+    J2, K2 = ref.jk_cart(dmc)
+    ref.close()
+    # both screens drop quartets below 1e-13 only
+    assert float((J1 - J2).abs().max()) < 1e-10
+    assert float((K1 - K2).abs().max()) < 1e-10
+    rj, rk = oracle.get_jk(mol, mf.dm.cpu().numpy())
+    J = (C.T @ J2[0] @ C).cpu().numpy()
+    K = (C.T @ K2[0] @ C).cpu().numpy()
+    assert abs(J - rj).max() < 1e-9
+    assert abs(K - rk).max() < 1e-9

@@ -130,3 +130,25 @@ def test_library_exports_header_symbols():
         assert hasattr(lib, n), n
     from byteqc_b200 import lib as L
     assert set(L.SYMBOLS) <= names
+
+
+@pytest.mark.parametrize('layout', ['q', 'shell', 'hybrid'])
+def test_tile_order_invariants(layout):
+    """Every pair once, padding with q = 0, q descending inside a tile and
+    along the tiles' first entries (what the host tile pruning relies on)."""
+    from byteqc_b200.scf.hf import _tile_order, PAIR_TILE
+    rng = np.random.default_rng(7)
+    for n in [0, 1, 5, 16, 17, 100, 1000]:
+        b = rng.integers(0, 20, n)
+        k = rng.integers(0, 50, n)
+        q = rng.random(n) ** 8
+        B, K, Q, D = _tile_order(b, k, q, layout)
+        assert len(B) % PAIR_TILE == 0
+        assert sorted(zip(B[~D], K[~D], Q[~D])) == sorted(zip(b, k, q))
+        assert np.all(Q[D] == 0)
+        T = Q.reshape(-1, PAIR_TILE)
+        assert np.all(np.diff(T, axis=1) <= 0)
+        assert np.all(np.diff(T[:, 0]) <= 0)
+        if layout == 'shell' and n:
+            Bt, Dt = B.reshape(-1, PAIR_TILE), D.reshape(-1, PAIR_TILE)
+            assert np.all((Bt == Bt[:, :1]) | Dt)
