@@ -42,12 +42,13 @@ __device__ __forceinline__ void rys_roots(const double *__restrict__ table, doub
         int k = (int)x;
         double t = 2.0 * (x - k) - 1.0;
         double t2 = t + t;
-        const double2 *c = reinterpret_cast<const double2 *>(
-            table + RYS_TABLE_OFFSET[N] + k * (RYS_NCOEF * 2 * N));
+        // level-major layout: (level kk, pair q) rows of XMAX[N] intervals
+        const int nint = RYS_XMAX[N];
+        const double2 *c = reinterpret_cast<const double2 *>(table + RYS_TABLE_OFFSET[N]) + k;
         double b1[2 * N], b2[2 * N];
 #pragma unroll
         for (int q = 0; q < N; q++) {
-            double2 v = __ldg(c + (RYS_NCOEF - 1) * N + q);
+            double2 v = __ldg(c + ((RYS_NCOEF - 1) * N + q) * nint);
             b1[2 * q] = v.x;
             b1[2 * q + 1] = v.y;
             b2[2 * q] = 0.0;
@@ -57,7 +58,7 @@ __device__ __forceinline__ void rys_roots(const double *__restrict__ table, doub
         for (int kk = RYS_NCOEF - 2; kk >= 1; kk--) {
 #pragma unroll
             for (int q = 0; q < N; q++) {
-                double2 v = __ldg(c + kk * N + q);
+                double2 v = __ldg(c + (kk * N + q) * nint);
                 double n0 = fma(t2, b1[2 * q], v.x - b2[2 * q]);
                 double n1 = fma(t2, b1[2 * q + 1], v.y - b2[2 * q + 1]);
                 b2[2 * q] = b1[2 * q];
@@ -68,7 +69,7 @@ __device__ __forceinline__ void rys_roots(const double *__restrict__ table, doub
         }
 #pragma unroll
         for (int q = 0; q < N; q++) {
-            double2 v = __ldg(c + q);
+            double2 v = __ldg(c + q * nint);
             double f0 = fma(t, b1[2 * q], v.x - b2[2 * q]);
             double f1 = fma(t, b1[2 * q + 1], v.y - b2[2 * q + 1]);
             // function index 2q and 2q+1: nodes are 0..N-1, weights N..2N-1
@@ -117,11 +118,13 @@ __device__ __forceinline__ double rys_one(const double *__restrict__ table, doub
         int k = (int)x;
         double t = 2.0 * (x - k) - 1.0;
         double t2 = t + t;
-        const double *c = table + RYS_TABLE_OFFSET[N] + k * (RYS_NCOEF * 2 * N) + q;
-        double b1 = __ldg(c + (RYS_NCOEF - 1) * 2 * N), b2 = 0.0;
+        const int nint = RYS_XMAX[N];
+        // element (level kk, pair q / 2, interval k, q % 2); level stride 2 N nint
+        const double *c = table + RYS_TABLE_OFFSET[N] + ((q >> 1) * nint + k) * 2 + (q & 1);
+        double b1 = __ldg(c + (RYS_NCOEF - 1) * 2 * N * nint), b2 = 0.0;
 #pragma unroll
         for (int kk = RYS_NCOEF - 2; kk >= 1; kk--) {
-            double n0 = fma(t2, b1, __ldg(c + kk * 2 * N) - b2);
+            double n0 = fma(t2, b1, __ldg(c + kk * 2 * N * nint) - b2);
             b2 = b1;
             b1 = n0;
         }

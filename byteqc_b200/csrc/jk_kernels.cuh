@@ -4,13 +4,16 @@
 // covers one block of the quartet space of a class pair: bra pairs
 // [a0, a0 + na) x ket pairs [b0, b0 + nb), cut into 16 x 16 tiles.  Each CTA
 // takes one tile, screens its 256 quartets on the device against
-// q_ij q_kl max|D| >= tol (the six density blocks a quartet touches), packs
-// the survivors into a shared-memory list and evaluates them:
+// q_ij q_kl max|D| >= tol (the six density blocks a quartet touches) and
+// evaluates the survivors:
 //
-// * jk_small: one thread per quartet for classes with at most SMALL_NF
-//   Cartesian components; the 2D integrals and the contracted quartet block
-//   live in registers and the six J/K targets are digested from registers.
-// * jk_group: TPQ = nfi * nfj * NSPLIT threads per quartet; thread
+// * jk_tile: one thread per quartet (16 x 16 threads per tile) for classes
+//   with at most SMALL_NF Cartesian components; the 2D integrals and the
+//   contracted quartet block live in registers, the six J/K targets are
+//   digested from registers with row / column / tile reductions where the
+//   tile's pairs share a target.
+// * jk_group: the survivors are packed into a shared-memory list and each
+//   takes TPQ = nfi * nfj * NSPLIT threads; thread
 //   (fi, fj, chunk) owns the ket components (fk in its chunk, all fl) of bra
 //   component (fi, fj).  Per primitive quartet the group evaluates the Rys
 //   roots and the per-root 2D tables (VRR + HRR) cooperatively into shared
@@ -147,174 +150,6 @@ __device__ __forceinline__ void load_prim(const JKArgs &A, const Quartet &Q, int
     P.x = aij * akl * P.inv_pq * rr;
     P.pref = Q.fac * eij * ekl / (aij * akl * sqrt(s));
 }
-
-// ---------------------------------------------------------------------------
-// thread-per-quartet kernel
-template <int LI, int LJ, int LK, int LL, typename F>
-__global__ void __launch_bounds__(256) jk_small(JKArgs A, JKTask T) {
-    constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = ncart(LK), NFL = ncart(LL);
-    constexpr int NF = NFI * NFJ * NFK * NFL;
-    constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
-    constexpr int GSZ = (LI + 1) * (LJ + 1) * (LK + 1) * (LL + 1);
-    __shared__ int s_list[TILE * TILE];
-    __shared__ int s_count;
-    int a_begin, b_begin, count;
-    if (!tile_screen(A, T, s_list, &s_count, a_begin, b_begin, count)) return;
-
-    for (int it = threadIdx.x; it < count; it += blockDim.x) {
-        int e = s_list[it];
-        Quartet Q;
-        load_quartet(A, a_begin + (e >> 16), b_begin + (e & 0xffff), Q);
-        F AB[3], CD[3];
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            AB[d] = F(Q.A[d] - Q.B[d]);
-            CD[d] = F(Q.C[d] - Q.D[d]);
-        }
-        F acc[NF];
-#pragma unroll
-        for (int n = 0; n < NF; n++) acc[n] = F(0);
-        int pa = T.pa0 + (Q.a - T.a0) * T.nprim_a;
-        int pb = T.pb0 + (Q.b - T.b0) * T.nprim_b;
-        for (int ip = 0; ip < T.nprim_a; ip++) {
-            for (int kp = 0; kp < T.nprim_b; kp++) {
-                PrimQuartet P;
-                load_prim(A, Q, pa + ip, pb + kp, P);
-                double rt[NR], wt[NR];
-                rys_roots<NR>(A.rys, P.x, rt, wt);
-#pragma unroll
-                for (int r = 0; r < NR; r++) {
-                    RootCoef c = root_coef(rt[r], P.p, P.q, P.inv_pq);
-                    F g[3][GSZ];
-#pragma unroll
-                    for (int d = 0; d < 3; d++) {
-                        F seed = (d == 2) ? F(wt[r] * P.pref) : F(1);
-                        gen_2d<LI, LJ, LK, LL, F>(seed, F(P.PA[d] - c.qs * P.PQ[d]),
-                                                  F(P.QC[d] + c.ps * P.PQ[d]), F(c.b00),
-                                                  F(c.b10), F(c.b01), AB[d], CD[d], g[d]);
-                    }
-#pragma unroll
-                    for (int fi = 0; fi < NFI; fi++)
-#pragma unroll
-                    for (int fj = 0; fj < NFJ; fj++)
-#pragma unroll
-                    for (int fk = 0; fk < NFK; fk++)
-#pragma unroll
-                    for (int fl = 0; fl < NFL; fl++) {
-                        constexpr int SJ = (LK + 1) * (LL + 1), SI = (LJ + 1) * SJ;
-                        int ix = cart_pow(LI, fi, 0) * SI + cart_pow(LJ, fj, 0) * SJ +
-                                 cart_pow(LK, fk, 0) * (LL + 1) + cart_pow(LL, fl, 0);
-                        int iy = cart_pow(LI, fi, 1) * SI + cart_pow(LJ, fj, 1) * SJ +
-                                 cart_pow(LK, fk, 1) * (LL + 1) + cart_pow(LL, fl, 1);
-                        int iz = cart_pow(LI, fi, 2) * SI + cart_pow(LJ, fj, 2) * SJ +
-                                 cart_pow(LK, fk, 2) * (LL + 1) + cart_pow(LL, fl, 2);
-                        int n = ((fi * NFJ + fj) * NFK + fk) * NFL + fl;
-                        acc[n] += g[0][ix] * g[1][iy] * g[2][iz];
-                    }
-                }
-            }
-        }
-        // digestion (FP64)
-        const int nao = A.nao;
-        const size_t nn = (size_t)nao * nao;
-        for (int id = 0; id < A.n_dm; id++) {
-            const double *__restrict__ D = A.dm + id * nn;
-            if (A.vj != nullptr) {
-                double *VJ = A.vj + id * nn;
-                double dkl[NFK * NFL], dij[NFI * NFJ];
-#pragma unroll
-                for (int fk = 0; fk < NFK; fk++)
-#pragma unroll
-                    for (int fl = 0; fl < NFL; fl++)
-                        dkl[fk * NFL + fl] = __ldg(D + (size_t)(Q.k0 + fk) * nao + Q.l0 + fl);
-#pragma unroll
-                for (int fi = 0; fi < NFI; fi++)
-#pragma unroll
-                    for (int fj = 0; fj < NFJ; fj++)
-                        dij[fi * NFJ + fj] = __ldg(D + (size_t)(Q.i0 + fi) * nao + Q.j0 + fj);
-#pragma unroll
-                for (int ij = 0; ij < NFI * NFJ; ij++) {
-                    double s = 0;
-#pragma unroll
-                    for (int kl = 0; kl < NFK * NFL; kl++) s += (double)acc[ij * NFK * NFL + kl] * dkl[kl];
-                    atomicAdd(VJ + (size_t)(Q.i0 + ij / NFJ) * nao + Q.j0 + ij % NFJ, s);
-                }
-#pragma unroll
-                for (int kl = 0; kl < NFK * NFL; kl++) {
-                    double s = 0;
-#pragma unroll
-                    for (int ij = 0; ij < NFI * NFJ; ij++) s += (double)acc[ij * NFK * NFL + kl] * dij[ij];
-                    atomicAdd(VJ + (size_t)(Q.k0 + kl / NFL) * nao + Q.l0 + kl % NFL, s);
-                }
-            }
-            if (A.vk != nullptr) {
-                double *VK = A.vk + id * nn;
-                double djl[NFJ][NFL], djk[NFJ][NFK], dil[NFI][NFL], dik[NFI][NFK];
-#pragma unroll
-                for (int fj = 0; fj < NFJ; fj++) {
-#pragma unroll
-                    for (int fl = 0; fl < NFL; fl++) djl[fj][fl] = __ldg(D + (size_t)(Q.j0 + fj) * nao + Q.l0 + fl);
-#pragma unroll
-                    for (int fk = 0; fk < NFK; fk++) djk[fj][fk] = __ldg(D + (size_t)(Q.j0 + fj) * nao + Q.k0 + fk);
-                }
-#pragma unroll
-                for (int fi = 0; fi < NFI; fi++) {
-#pragma unroll
-                    for (int fl = 0; fl < NFL; fl++) dil[fi][fl] = __ldg(D + (size_t)(Q.i0 + fi) * nao + Q.l0 + fl);
-#pragma unroll
-                    for (int fk = 0; fk < NFK; fk++) dik[fi][fk] = __ldg(D + (size_t)(Q.i0 + fi) * nao + Q.k0 + fk);
-                }
-#define ACC(fi, fj, fk, fl) ((double)acc[(((fi) * NFJ + (fj)) * NFK + (fk)) * NFL + (fl)])
-#pragma unroll
-                for (int fi = 0; fi < NFI; fi++)
-#pragma unroll
-                    for (int fk = 0; fk < NFK; fk++) {
-                        double s = 0;
-#pragma unroll
-                        for (int fj = 0; fj < NFJ; fj++)
-#pragma unroll
-                            for (int fl = 0; fl < NFL; fl++) s += ACC(fi, fj, fk, fl) * djl[fj][fl];
-                        atomicAdd(VK + (size_t)(Q.i0 + fi) * nao + Q.k0 + fk, s);
-                    }
-#pragma unroll
-                for (int fi = 0; fi < NFI; fi++)
-#pragma unroll
-                    for (int fl = 0; fl < NFL; fl++) {
-                        double s = 0;
-#pragma unroll
-                        for (int fj = 0; fj < NFJ; fj++)
-#pragma unroll
-                            for (int fk = 0; fk < NFK; fk++) s += ACC(fi, fj, fk, fl) * djk[fj][fk];
-                        atomicAdd(VK + (size_t)(Q.i0 + fi) * nao + Q.l0 + fl, s);
-                    }
-#pragma unroll
-                for (int fj = 0; fj < NFJ; fj++)
-#pragma unroll
-                    for (int fk = 0; fk < NFK; fk++) {
-                        double s = 0;
-#pragma unroll
-                        for (int fi = 0; fi < NFI; fi++)
-#pragma unroll
-                            for (int fl = 0; fl < NFL; fl++) s += ACC(fi, fj, fk, fl) * dil[fi][fl];
-                        atomicAdd(VK + (size_t)(Q.j0 + fj) * nao + Q.k0 + fk, s);
-                    }
-#pragma unroll
-                for (int fj = 0; fj < NFJ; fj++)
-#pragma unroll
-                    for (int fl = 0; fl < NFL; fl++) {
-                        double s = 0;
-#pragma unroll
-                        for (int fi = 0; fi < NFI; fi++)
-#pragma unroll
-                            for (int fk = 0; fk < NFK; fk++) s += ACC(fi, fj, fk, fl) * dik[fi][fk];
-                        atomicAdd(VK + (size_t)(Q.j0 + fj) * nao + Q.l0 + fl, s);
-                    }
-#undef ACC
-            }
-        }
-    }
-}
-
 
 // ---------------------------------------------------------------------------
 // fixed-layout tile kernel: thread (row, col) of a 256-thread CTA evaluates
@@ -748,6 +583,9 @@ jk_group(JKArgs A, JKTask T) {
                         int r = task / 3, d = task % 3;
                         RootCoef c = root_coef(rw[r], P.p, P.q, P.inv_pq);
                         double seed = (d == 2) ? rw[NR + r] * P.pref : 1.0;
+                        // d is a runtime index, so P and AB/CD sit in local memory
+                        // (L1): measured faster than selecting from registers,
+                        // which raises the register count of the whole kernel
                         gen_2d<LI, LJ, LK, LL, F>(F(seed), F(P.PA[d] - c.qs * P.PQ[d]),
                                                   F(P.QC[d] + c.ps * P.PQ[d]), F(c.b00), F(c.b10),
                                                   F(c.b01), F(AB[d]), F(CD[d]),
@@ -940,14 +778,19 @@ static inline int task_tiles(const JKTask &task) {
     return ((task.na + TILE - 1) / TILE) * ((task.nb + TILE - 1) / TILE);
 }
 
+template <int LI, int LJ, int LK, int LL, typename F>
+static void launch_tile_f(const JKArgs &args, const JKTask &task, int ntiles, cudaStream_t stream) {
+    jk_tile<LI, LJ, LK, LL, F><<<ntiles, 256, 0, stream>>>(args, task);
+}
+
 template <int LI, int LJ, int LK, int LL>
 static int launch_small(const JKArgs &args, const JKTask &task, int fp32, cudaStream_t stream) {
     int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
     if (ntiles == 0) return 0;
     if (fp32)
-        jk_tile<LI, LJ, LK, LL, float><<<ntiles, 256, 0, stream>>>(args, task);
+        launch_tile_f<LI, LJ, LK, LL, float>(args, task, ntiles, stream);
     else
-        jk_tile<LI, LJ, LK, LL, double><<<ntiles, 256, 0, stream>>>(args, task);
+        launch_tile_f<LI, LJ, LK, LL, double>(args, task, ntiles, stream);
     return 0;
 }
 

@@ -162,8 +162,10 @@ def main():
     lines.append('// Generated by byteqc_b200/rys/gen_rys_tables.py; do not edit.')
     lines.append('// Rys nodes s=t^2 and weights: degree-%d Chebyshev series on unit' % DEG)
     lines.append('// intervals of x in [0, XMAX[n]); Gauss-Hermite limit beyond.')
-    lines.append('// Layout per (n, interval): [coef k = 0..%d][q = 0..2n-1],' % DEG)
-    lines.append('// q < n: nodes in ascending order, q >= n: weights.')
+    lines.append('// Layout per n: [coef k = 0..%d][pair p = 0..n-1][interval a = 0..XMAX[n]-1]' % DEG)
+    lines.append('// [2]: functions q = 2p and 2p+1 of interval a (q < n: nodes in ascending')
+    lines.append('// order, q >= n: weights).  Level-major, so that the lanes of a warp that')
+    lines.append('// evaluate different intervals read neighbouring addresses.')
     lines.append('#define RYS_NMAX %d' % NMAX)
     lines.append('#define RYS_NCOEF %d' % (DEG + 1))
     lines.append('// The including file defines RYS_CONST (storage of the big table) and')
@@ -178,13 +180,14 @@ def main():
     lines.append('#ifndef RYS_NO_BIG_TABLE')
     lines.append('RYS_CONST double RYS_TABLE[%d] = {' % offs[-1])
     for n in range(1, NMAX + 1):
-        for a in range(xmax[n]):
-            coefs = table[(n, a)]
-            vals = []
-            for k in range(DEG + 1):
-                for q in range(2 * n):
-                    vals.append('%.17g' % coefs[q][k])
-            lines.append('  ' + ', '.join(vals) + ',')
+        for k in range(DEG + 1):
+            for p in range(n):
+                vals = []
+                for a in range(xmax[n]):
+                    coefs = table[(n, a)]
+                    vals.append('%.17g' % coefs[2 * p][k])
+                    vals.append('%.17g' % coefs[2 * p + 1][k])
+                lines.append('  ' + ', '.join(vals) + ',')
     lines.append('};')
     lines.append('#endif')
     hoffs = [0]

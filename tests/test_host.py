@@ -104,7 +104,8 @@ def test_committed_rys_table_against_mpmath():
         if x < xmax[n]:
             k = int(x)
             t = 2 * (x - k) - 1
-            c = tab[off[n] + k * 12 * 2 * n: off[n] + (k + 1) * 12 * 2 * n].reshape(12, 2 * n)
+            # level-major: [level][pair][interval][2]
+            c = tab[off[n]:off[n + 1]].reshape(12, n, xmax[n], 2)[:, :, k, :].reshape(12, 2 * n)
             b1 = c[11].copy()
             b2 = np.zeros(2 * n)
             for kk in range(10, 0, -1):
