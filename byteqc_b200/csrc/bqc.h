@@ -22,7 +22,8 @@ struct JKArgs {
     double tol;               // drop quartets with q_ij q_kl max|D| < tol
     double tol_hi;            // and, when > 0, those with a bound >= tol_hi (FP32 band)
     int *status;              // device error word (0 = ok), may be NULL
-    const double *rys;        // Rys coefficient table (bqc_rys_table())
+    const double *rys;        // Rys coefficient table, interval-major (bqc_rys_table())
+    const double *rys_lm;     // the same, level-major (bqc_rys_table_lm())
 };
 
 // One rectangular (or triangular, when diag) block of the quartet space.
@@ -51,6 +52,7 @@ unsigned long long bqc_count_launch(int n);
 
 // device address of the Rys coefficient table on the current device (rys_table.cu)
 const double *bqc_rys_table();
+const double *bqc_rys_table_lm();
 
 // launchers (jk_dispatch.cu, schwarz.cu)
 int bqc_launch_jk(int li, int lj, int lk, int ll, const JKArgs &args, const JKTask &task,

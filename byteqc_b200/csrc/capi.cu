@@ -151,6 +151,7 @@ static JKArgs make_args(const BasisProdCache *bp, double *vj, double *vk, const 
     a.nbas = bp->nbas;
     a.n_dm = n_dm;
     a.rys = bqc_rys_table();
+    a.rys_lm = bqc_rys_table_lm();
     return a;
 }
 

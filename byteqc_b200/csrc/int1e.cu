@@ -177,7 +177,7 @@ using namespace bqc;
 extern "C" int BQCint1e(const int *atm, int natm, const int *bas, int nbas, const double *env,
                         const int *ao_loc, int nao, double *S, double *T, double *V,
                         cudaStream_t stream) {
-    const double *rys = bqc_rys_table();
+    const double *rys = bqc_rys_table_lm();
     if (rys == nullptr) return 1;
     // group shell pairs (ish >= jsh, l_i >= l_j after ordering) by class on the host
     std::vector<int> hbas(nbas * BAS_SLOTS);

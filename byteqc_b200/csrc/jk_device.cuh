@@ -14,6 +14,9 @@
 
 namespace bqc {
 
+// number of unit intervals of the order-n table (compile-time copy of RYS_XMAX)
+constexpr int kRysXmax[RYS_NMAX + 1] = {RYS_XMAX_LIST};
+
 __host__ __device__ constexpr int ncart(int l) { return (l + 1) * (l + 2) / 2; }
 __host__ __device__ constexpr int imax(int a, int b) { return a > b ? a : b; }
 __host__ __device__ constexpr int imin(int a, int b) { return a < b ? a : b; }
@@ -35,15 +38,17 @@ __host__ __device__ constexpr int cart_pow(int l, int c, int d) {
 
 // Rys nodes s = t^2 and weights of order N at x, FP64, from the fitted tables
 // (Chebyshev series on unit intervals, Gauss-Hermite limit beyond XMAX).
+// table is the level-major copy (RYS_TABLE_LM): the lanes of a warp hold
+// different x and read neighbouring addresses.
 template <int N>
 __device__ __forceinline__ void rys_roots(const double *__restrict__ table, double x,
                                           double *__restrict__ r, double *__restrict__ w) {
-    if (x < (double)RYS_XMAX[N]) {
+    constexpr int nint = kRysXmax[N];
+    if (x < (double)nint) {
         int k = (int)x;
         double t = 2.0 * (x - k) - 1.0;
         double t2 = t + t;
         // level-major layout: (level kk, pair q) rows of XMAX[N] intervals
-        const int nint = RYS_XMAX[N];
         const double2 *c = reinterpret_cast<const double2 *>(table + RYS_TABLE_OFFSET[N]) + k;
         double b1[2 * N], b2[2 * N];
 #pragma unroll
@@ -111,20 +116,21 @@ __device__ __forceinline__ void rys_roots1(double x, double &s, double &w) {
     s = f1 / f0;
 }
 
-// One function of the order-N rule (q < N: node q, q >= N: weight q - N).
+// One function of the order-N rule (q < N: node q, q >= N: weight q - N),
+// from the interval-major table (the lanes that call it for one x read the
+// same interval).
 template <int N>
 __device__ __forceinline__ double rys_one(const double *__restrict__ table, double x, int q) {
-    if (x < (double)RYS_XMAX[N]) {
+    constexpr int nint = kRysXmax[N];
+    if (x < (double)nint) {
         int k = (int)x;
         double t = 2.0 * (x - k) - 1.0;
         double t2 = t + t;
-        const int nint = RYS_XMAX[N];
-        // element (level kk, pair q / 2, interval k, q % 2); level stride 2 N nint
-        const double *c = table + RYS_TABLE_OFFSET[N] + ((q >> 1) * nint + k) * 2 + (q & 1);
-        double b1 = __ldg(c + (RYS_NCOEF - 1) * 2 * N * nint), b2 = 0.0;
+        const double *c = table + RYS_TABLE_OFFSET[N] + k * (RYS_NCOEF * 2 * N) + q;
+        double b1 = __ldg(c + (RYS_NCOEF - 1) * 2 * N), b2 = 0.0;
 #pragma unroll
         for (int kk = RYS_NCOEF - 2; kk >= 1; kk--) {
-            double n0 = fma(t2, b1, __ldg(c + kk * 2 * N * nint) - b2);
+            double n0 = fma(t2, b1, __ldg(c + kk * 2 * N) - b2);
             b2 = b1;
             b1 = n0;
         }

@@ -266,7 +266,7 @@ __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
                 load_prim(A, Q, pa + ip, pb + kp, P);
                 double rt[NR], wt[NR];
                 if constexpr (NR == 1) rys_roots1(P.x, rt[0], wt[0]);
-                else rys_roots<NR>(A.rys, P.x, rt, wt);
+                else rys_roots<NR>(A.rys_lm, P.x, rt, wt);
 #pragma unroll
                 for (int rr = 0; rr < NR; rr++) {
                     RootCoef cf = root_coef(rt[rr], P.p, P.q, P.inv_pq);

@@ -15,3 +15,9 @@ const double *bqc_rys_table() {
     if (cudaGetSymbolAddress(&ptr, RYS_TABLE) != cudaSuccess) return nullptr;
     return static_cast<const double *>(ptr);
 }
+
+const double *bqc_rys_table_lm() {
+    void *ptr = nullptr;
+    if (cudaGetSymbolAddress(&ptr, RYS_TABLE_LM) != cudaSuccess) return nullptr;
+    return static_cast<const double *>(ptr);
+}

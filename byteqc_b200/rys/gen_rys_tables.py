@@ -162,16 +162,22 @@ def main():
     lines.append('// Generated by byteqc_b200/rys/gen_rys_tables.py; do not edit.')
     lines.append('// Rys nodes s=t^2 and weights: degree-%d Chebyshev series on unit' % DEG)
     lines.append('// intervals of x in [0, XMAX[n]); Gauss-Hermite limit beyond.')
-    lines.append('// Layout per n: [coef k = 0..%d][pair p = 0..n-1][interval a = 0..XMAX[n]-1]' % DEG)
-    lines.append('// [2]: functions q = 2p and 2p+1 of interval a (q < n: nodes in ascending')
-    lines.append('// order, q >= n: weights).  Level-major, so that the lanes of a warp that')
-    lines.append('// evaluate different intervals read neighbouring addresses.')
+    lines.append('// Two layouts of the same coefficients:')
+    lines.append('// RYS_TABLE, interval-major: per (n, interval a) [coef k = 0..%d][q = 0..2n-1];' % DEG)
+    lines.append('//   the functions of one x are contiguous (several lanes evaluating')
+    lines.append('//   different functions of one x read one line).')
+    lines.append('// RYS_TABLE_LM, level-major: per n [k][pair p = 0..n-1][a = 0..XMAX[n]-1][2]')
+    lines.append('//   holding functions q = 2p, 2p+1 (lanes evaluating the same functions of')
+    lines.append('//   different x read neighbouring addresses).')
+    lines.append('// q < n: nodes s = t^2 in ascending order, q >= n: weights.')
     lines.append('#define RYS_NMAX %d' % NMAX)
     lines.append('#define RYS_NCOEF %d' % (DEG + 1))
     lines.append('// The including file defines RYS_CONST (storage of the big table) and')
     lines.append('// RYS_CONST_SMALL (storage of the small index tables).')
     lines.append('RYS_CONST_SMALL int RYS_XMAX[%d] = {0, %s};' % (
         NMAX + 1, ', '.join(str(xmax[n]) for n in range(1, NMAX + 1))))
+    lines.append('// the same list for compile-time use (strides of the level-major layout)')
+    lines.append('#define RYS_XMAX_LIST 0, %s' % ', '.join(str(xmax[n]) for n in range(1, NMAX + 1)))
     offs = [0]
     for n in range(1, NMAX + 1):
         offs.append(offs[-1] + xmax[n] * (DEG + 1) * 2 * n)
@@ -179,6 +185,16 @@ def main():
         NMAX + 2, ', '.join(str(o) for o in offs)))
     lines.append('#ifndef RYS_NO_BIG_TABLE')
     lines.append('RYS_CONST double RYS_TABLE[%d] = {' % offs[-1])
+    for n in range(1, NMAX + 1):
+        for a in range(xmax[n]):
+            coefs = table[(n, a)]
+            vals = []
+            for k in range(DEG + 1):
+                for q in range(2 * n):
+                    vals.append('%.17g' % coefs[q][k])
+            lines.append('  ' + ', '.join(vals) + ',')
+    lines.append('};')
+    lines.append('RYS_CONST double RYS_TABLE_LM[%d] = {' % offs[-1])
     for n in range(1, NMAX + 1):
         for k in range(DEG + 1):
             for p in range(n):

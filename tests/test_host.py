@@ -90,13 +90,13 @@ def _table():
         m = re.search(r'%s\[\d+\] = \{(.*?)\};' % name, src, re.S)
         return np.array([typ(v) for v in m.group(1).replace('\n', ' ').split(',') if v.strip()])
     return (arr('RYS_XMAX', int), arr('RYS_TABLE_OFFSET', int), arr('RYS_TABLE'),
-            arr('RYS_HERM_OFFSET', int), arr('RYS_HERM_R2'), arr('RYS_HERM_W'))
+            arr('RYS_HERM_OFFSET', int), arr('RYS_HERM_R2'), arr('RYS_HERM_W'), arr('RYS_TABLE_LM'))
 
 
 def test_committed_rys_table_against_mpmath():
     """Clenshaw evaluation of the committed table, restated in numpy, matches
     the 60-digit golden values."""
-    xmax, off, tab, hoff, hr2, hw = _table()
+    xmax, off, tab, hoff, hr2, hw, tab_lm = _table()
     data = json.load(open(os.path.join(ROOT, 'tests', 'golden', 'rys_mpmath.json')))
     worst = 0
     for rec in data:
@@ -104,8 +104,10 @@ def test_committed_rys_table_against_mpmath():
         if x < xmax[n]:
             k = int(x)
             t = 2 * (x - k) - 1
-            # level-major: [level][pair][interval][2]
-            c = tab[off[n]:off[n + 1]].reshape(12, n, xmax[n], 2)[:, :, k, :].reshape(12, 2 * n)
+            c = tab[off[n] + k * 12 * 2 * n: off[n] + (k + 1) * 12 * 2 * n].reshape(12, 2 * n)
+            # the level-major copy holds the same coefficients
+            lm = tab_lm[off[n]:off[n + 1]].reshape(12, n, xmax[n], 2)[:, :, k, :].reshape(12, 2 * n)
+            assert np.array_equal(c, lm)
             b1 = c[11].copy()
             b2 = np.zeros(2 * n)
             for kk in range(10, 0, -1):
