@@ -11,7 +11,10 @@ dominant J/K kernel class of one full J+K build with the converged density.
 
 --impl reference: the CPU oracle (OpenMP C restatement of the reference's
 get_jk path) on the host cores, on a bounded sample of the same workload,
-projected to the workload by the algorithmic FLOP count.
+projected to the workload by the algorithmic FLOP count; beside it
+(``reference_gpu``) one J/K build of the workload by the reference's own GPU
+kernels (oracle/_ref) on the same GPU, which the main line's ``jk_build``
+repeats with this engine on the same density.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -106,7 +109,7 @@ class ClockSampler:
                 'samples': len(self.rows)}
 
 
-FP32_BELOW = 1e-6   # bound below which the fast form evaluates quartets in FP32
+FP32_BELOW = 1e-4   # bound below which the fast form evaluates quartets in FP32
 EARLY_TOL = 1e-10   # screening threshold of the fast form before its final FP64 rebuild
 
 
@@ -321,6 +324,11 @@ def main():
                                  'to the %.3g FLOP of the workload SCF' % (f_s, t_s, ref['scf_flops'])},
                 'e2e': {'value': round(value, 2), 'unit': 's', 'h2d_bytes_per_step': 0,
                         'd2h_bytes_per_step': 0}}
+        # the reference's own GPU kernels on the same GPU, one J/K build
+        try:
+            line['reference_gpu'] = reference_gpu_build(mol_full)
+        except Exception as exc:   # report, never fail the CPU line
+            line['reference_gpu'] = {'unavailable': '%s: %s' % (type(exc).__name__, exc)}
         print(json.dumps(line))
         return
 
@@ -398,6 +406,12 @@ def main():
                        'energy_diff_vs_device_loop': abs(e_h - e)}
         peak = ctypes_peak(lib)
         line['roofline'] = roofline(mf, peak)
+        # one J/K build on the density of the reference's timing script (the
+        # reference arm times its own kernels on the same one)
+        opt = mf.opt
+        dmc = jkpy_density(opt)
+        line['jk_build'] = {'s': round(time_build(lambda: opt.jk_cart(dmc)), 3),
+                            'density': JKPY_DENSITY, 'tol': opt.direct_scf_tol}
         # FLOPs of the J/K builds of a plain-FP64 solve: the CPU projection's
         # numerator (recorded per workload; --account recounts on the device)
         key = '(H2O)%d/%s' % (args.nwater, args.basis)
@@ -421,6 +435,60 @@ def main():
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+JKPY_DENSITY = 'random symmetric AO density (rand + rand^T) x 0.1, seed 2341'
+
+
+def jkpy_density(opt):
+    """The density of the reference's J/K timing script (cuobc/test/jk.py),
+    in the internal Cartesian basis of opt."""
+    import torch
+    rng = np.random.default_rng(2341)
+    n0 = opt.coeff.shape[1]
+    dm = rng.random((n0, n0))
+    dm = torch.as_tensor(0.1 * (dm + dm.T), device='cuda')
+    C = opt.coeff_dev
+    return (C @ dm @ C.T)[None].contiguous()
+
+
+def time_build(fn, reps=2):
+    """Shortest of reps CUDA-event timed calls after one warm-up call (s)."""
+    import torch
+    fn()
+    best = 1e30
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        fn()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    return best
+
+
+def reference_gpu_build(mol):
+    """Seconds of one J/K build by the reference's own GPU kernels (oracle/_ref,
+    compiled from cuobc/lib for sm_100a) on the jk.py density, or a reason."""
+    import torch
+    from oracle import ref_gpu
+    if not torch.cuda.is_available():
+        return {'unavailable': 'no GPU'}
+    if not ref_gpu.available():
+        return {'unavailable': 'oracle/_ref not built (the reference sources were absent at build time)'}
+    from byteqc_b200.scf import hf
+    opt = hf._VHFOpt(mol).build()
+    ref = ref_gpu.RefJK(opt)
+    dmc = jkpy_density(opt)
+    tasks = ref.tasks(dmc)
+    t = time_build(lambda: ref.jk_cart(dmc, tasks=tasks), reps=1)
+    ref.close()
+    return {'jk_build_s': round(t, 3), 'density': JKPY_DENSITY, 'launches': len(tasks),
+            'what': 'GINTbuild_jk of the reference (cuobc/lib/gvhf, cuobc/lib/gint) built for '
+                    'sm_100a, driven by the restated host logic of cuobc/scf/hf.py get_jk '
+                    '(log-q bins, class-level density screen); same B200, CUDA events'}
 
 
 def ctypes_peak(lib):

@@ -588,11 +588,11 @@ class RHF(_SCFBase):
     pyscf's direct SCF (a full rebuild every ``rebuild_cycle`` cycles when it
     is positive; by default only the first build is a full one).
 
-    Mixed precision (``fp32_threshold > 0``): on the incremental builds the
-    quartets whose bound q_ij q_kl max|dD| is below fp32_threshold are
-    evaluated in FP32 (roots, weights, Fock accumulation stay FP64), and with
-    ``early_tol`` > direct_scf_tol those builds also drop quartets below
-    early_tol.  Once |Delta E| < ``mixed_switch_tol`` the Fock matrix is
+    Mixed precision (``fp32_threshold > 0``): on the builds before the switch
+    (the first, full one and the incremental ones) the quartets whose bound
+    q_ij q_kl max|D| is below fp32_threshold are evaluated in FP32 (roots,
+    weights, Fock accumulation stay FP64), and with ``early_tol`` >
+    direct_scf_tol those builds also drop quartets below early_tol.  Once |Delta E| < ``mixed_switch_tol`` the Fock matrix is
     rebuilt in full in FP64 at direct_scf_tol and the remaining cycles are
     FP64 incremental builds at direct_scf_tol; convergence is only accepted
     between two such final cycles, so the converged energy is an FP64 energy.
@@ -643,13 +643,16 @@ class RHF(_SCFBase):
             tj = time.perf_counter()
             full = dm_last is None or (self.rebuild_cycle > 0 and cycle % self.rebuild_cycle == 0) \
                 or (mixed and final and n_final == 0)
-            fp32_below = 0. if (final or full) else self.fp32_threshold
+            # before the switch every build, the first full one included, takes
+            # the FP32 band and the early screen: the full FP64 rebuild at the
+            # switch replaces all of it
+            fp32_below = 0. if final else self.fp32_threshold
             tol = opt.direct_scf_tol
-            if mixed and not final and not full:
+            if mixed and not final:
                 tol = max(tol, self.early_tol)
             if full:
                 dm_in = dm
-                vj, vk = opt.jk_ao(dm[None])
+                vj, vk = opt.jk_ao(dm[None], fp32_below=fp32_below, tol=tol)
             else:
                 dm_in = dm - dm_last
                 dvj, dvk = opt.jk_ao(dm_in[None], fp32_below=fp32_below, tol=tol)
@@ -728,12 +731,13 @@ class RHF(_SCFBase):
         for cycle in range(self.max_cycle):
             full = dm_last is None or (self.rebuild_cycle > 0 and cycle % self.rebuild_cycle == 0) \
                 or (mixed and final and n_final == 0)
+            fp32_below = 0. if final else self.fp32_threshold
+            tol = None if final else max(self.opt.direct_scf_tol, self.early_tol)
             if full:
-                vj, vk = get_jk(self.mol, dm, 1, self.opt)
+                vj, vk = get_jk(self.mol, dm, 1, self.opt, fp32_below=fp32_below, tol=tol)
             else:
-                dvj, dvk = get_jk(self.mol, dm - dm_last, 1, self.opt,
-                                  fp32_below=0. if final else self.fp32_threshold,
-                                  tol=None if final else max(self.opt.direct_scf_tol, self.early_tol))
+                dvj, dvk = get_jk(self.mol, dm - dm_last, 1, self.opt, fp32_below=fp32_below,
+                                  tol=tol)
                 vj, vk = vj + dvj, vk + dvk
             h2d += dm.nbytes
             d2h += 2 * dm.nbytes
