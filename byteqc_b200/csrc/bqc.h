@@ -50,6 +50,12 @@ struct JKTask {
 // number of kernel launches issued by the library so far (all threads)
 unsigned long long bqc_count_launch(int n);
 
+// launch variant of a class (canonical order), see launch_class
+#define BQC_VARIANT_AUTO 0
+#define BQC_VARIANT_GROUP 1
+#define BQC_VARIANT_SPLIT 2
+int bqc_class_variant(int li, int lj, int lk, int ll);
+
 // device address of the Rys coefficient table on the current device (rys_table.cu)
 const double *bqc_rys_table();
 const double *bqc_rys_table_lm();

@@ -19,6 +19,25 @@ unsigned long long bqc_count_launch(int n) { return __atomic_add_fetch(&g_launch
 
 extern "C" unsigned long long BQClaunch_counter(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
+// launch variant per canonical class (li >= lj, lk >= ll, bra pair index >=
+// ket pair index); written by BQCset_class_variant, read at every launch
+static int g_variant[BQC_LMAX + 1][BQC_LMAX + 1][BQC_LMAX + 1][BQC_LMAX + 1];
+
+int bqc_class_variant(int li, int lj, int lk, int ll) { return g_variant[li][lj][lk][ll]; }
+
+extern "C" int BQCset_class_variant(int li, int lj, int lk, int ll, int variant) {
+    if (variant < BQC_VARIANT_AUTO || variant > BQC_VARIANT_SPLIT) return 3;
+    if (li < lj) std::swap(li, lj);
+    if (lk < ll) std::swap(lk, ll);
+    if (li < 0 || lj < 0 || lk < 0 || ll < 0 || li > BQC_LMAX || lk > BQC_LMAX) return 2;
+    if (li * (li + 1) / 2 + lj < lk * (lk + 1) / 2 + ll) {
+        std::swap(li, lk);
+        std::swap(lj, ll);
+    }
+    g_variant[li][lj][lk][ll] = variant;
+    return 0;
+}
+
 int bqc_launch_jk(int li, int lj, int lk, int ll, const JKArgs &args, const JKTask &task,
                   int fp32, cudaStream_t stream) {
     bqc_count_launch(1);

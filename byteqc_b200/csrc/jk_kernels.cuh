@@ -45,17 +45,24 @@ __device__ __forceinline__ double dmax6(const double *__restrict__ dmc, int nbas
     return fmax(m, __ldg(dmc + j * nbas + l));
 }
 
-__device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, int *s_list,
-                                            int *s_count, int &a_begin, int &b_begin,
-                                            int &count) {
-    int r, c;
+// Tile (row r, column c) of this block.  With tile_prefix (tile_prefix[r] =
+// first block of tile row r, non-decreasing) the row is the largest r with
+// tile_prefix[r] <= blockIdx.x, found by a 32-way search: each round every
+// lane of the warp tests one of 32 evenly spaced candidates and a ballot
+// keeps the last one that qualifies, so a row index of up to 2^20 takes four
+// rounds of loads instead of twenty dependent ones.  All 32 lanes of every
+// warp must call it.
+__device__ __forceinline__ void tile_of_block(const JKTask &T, int &r, int &c) {
     if (T.tile_prefix != nullptr) {
-        // largest r with tile_prefix[r] <= blockIdx.x
-        int lo = 0, hi = T.nrows - 1;
-        const int x = blockIdx.x;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (__ldg(T.tile_prefix + mid) <= x) lo = mid; else hi = mid - 1;
+        const int x = blockIdx.x, lane = threadIdx.x & 31;
+        int lo = 0, hi = T.nrows;   // tile_prefix[lo] <= x; answer in [lo, hi)
+        while (hi - lo > 1) {
+            const int step = (hi - lo + 31) >> 5;
+            const int idx = lo + lane * step;
+            const bool le = idx < hi && __ldg(T.tile_prefix + idx) <= x;
+            const unsigned m = __ballot_sync(0xffffffffu, le);   // bit 0 always set
+            lo += (31 - __clz(m)) * step;
+            hi = min(hi, lo + step);
         }
         r = lo;
         c = x - __ldg(T.tile_prefix + r);
@@ -65,6 +72,13 @@ __device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, in
         r = blockIdx.x / ncols;
         c = blockIdx.x % ncols;
     }
+}
+
+__device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, int *s_list,
+                                            int *s_count, int &a_begin, int &b_begin,
+                                            int &count) {
+    int r, c;
+    tile_of_block(T, r, c);
     int ta = T.rows_are_b ? c : r, tb = T.rows_are_b ? r : c;
     a_begin = T.a0 + ta * TILE;
     b_begin = T.b0 + tb * TILE;
@@ -176,51 +190,53 @@ __device__ __forceinline__ void row_reduce(double (&v)[NV]) {
 
 // Sum v over the 16 rows of the tile for each column; afterwards threads
 // call emit(col, n, sum) for the 16 * NV results.  Every thread must call.
+// The shared buffer holds NRED values per (warp, column); longer vectors go
+// through it in blocks of NRED.
 template <int NV, int NRED, typename Emit>
 __device__ __forceinline__ void col_reduce(double (&v)[NV], double (*s_red)[16][NRED], Emit emit) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-    for (int n = 0; n < NV; n++) {
-        double x = v[n] + __shfl_xor_sync(0xffffffffu, v[n], 16);
-        if (lane < 16) s_red[warp][lane][n] = x;
-    }
-    __syncthreads();
-    for (int o = threadIdx.x; o < 16 * NV; o += blockDim.x) {
-        int cc = o / NV, n = o % NV;
-        double s = 0;
+    for (int n0 = 0; n0 < NV; n0 += NRED) {
+        constexpr int NB = NV < NRED ? NV : NRED;
 #pragma unroll
-        for (int w = 0; w < 8; w++) s += s_red[w][cc][n];
-        emit(cc, n, s);
+        for (int m = 0; m < NB; m++) {
+            if (n0 + m < NV) {
+                double x = v[n0 + m] + __shfl_xor_sync(0xffffffffu, v[n0 + m], 16);
+                if (lane < 16) s_red[warp][lane][m] = x;
+            }
+        }
+        __syncthreads();
+        const int nb = imin(NRED, NV - n0);
+        for (int o = threadIdx.x; o < 16 * nb; o += blockDim.x) {
+            int cc = o / nb, m = o % nb;
+            double s = 0;
+#pragma unroll
+            for (int w = 0; w < 8; w++) s += s_red[w][cc][m];
+            emit(cc, n0 + m, s);
+        }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
-template <int LI, int LJ, int LK, int LL, typename F>
+// K0, KN: the launch evaluates the ket components fk in [K0, K0 + KN) of shell
+// k only (all of them by default).  Every J/K target is linear in the quartet
+// block, so launches over disjoint fk ranges add up to the whole class; a
+// class too large for one thread's registers runs as a few such launches.
+template <int LI, int LJ, int LK, int LL, typename F, int K0 = 0, int KN = ncart(LK)>
 __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
-    constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = ncart(LK), NFL = ncart(LL);
+    static_assert(K0 >= 0 && KN >= 1 && K0 + KN <= ncart(LK), "ket component range");
+    // NFK: the components of shell k this launch evaluates, from K0 on
+    constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = KN, NFL = ncart(LL);
     constexpr int NIJ = NFI * NFJ, NKL = NFK * NFL, NF = NIJ * NKL;
     constexpr int NR = (LI + LJ + LK + LL) / 2 + 1;
     constexpr int GSZ = (LI + 1) * (LJ + 1) * (LK + 1) * (LL + 1);
-    constexpr int NRED = imax(NKL, imax(NFI * NFL, NFI * NFK));
+    // column-reduction buffer: at most 32 values per (warp, column), 32 KB
+    constexpr int NRED = imin(32, imax(NKL, imax(NFI * NFL, NFI * NFK)));
     __shared__ double s_red[8][16][NRED];
 
     // tile of this block
     int r, c;
-    if (T.tile_prefix != nullptr) {
-        int lo = 0, hi = T.nrows - 1;
-        const int x = blockIdx.x;
-        while (lo < hi) {
-            int mid = (lo + hi + 1) >> 1;
-            if (__ldg(T.tile_prefix + mid) <= x) lo = mid; else hi = mid - 1;
-        }
-        r = lo;
-        c = x - __ldg(T.tile_prefix + r);
-        if (T.tile_col0 != nullptr) c += __ldg(T.tile_col0 + r);
-    } else {
-        int ncols = ((T.rows_are_b ? T.na : T.nb) + TILE - 1) / TILE;
-        r = blockIdx.x / ncols;
-        c = blockIdx.x % ncols;
-    }
+    tile_of_block(T, r, c);
     const int ta = T.rows_are_b ? c : r, tb = T.rows_are_b ? r : c;
     const int a_begin = T.a0 + ta * TILE, b_begin = T.b0 + tb * TILE;
     const int a_end = min(T.a0 + T.na, a_begin + TILE), b_end = min(T.b0 + T.nb, b_begin + TILE);
@@ -240,6 +256,7 @@ __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
     Quartet Q;
     if (active) {
         load_quartet(A, a, b, Q);
+        Q.k0 += K0;   // first AO of the evaluated k components
         if (A.pair_q != nullptr) {
             double bound = __ldg(A.pair_q + a) * __ldg(A.pair_q + b);
             if (A.dm_cond != nullptr) bound *= dmax6(A.dm_cond, A.nbas, Q.ish, Q.jsh, Q.ksh, Q.lsh);
@@ -288,11 +305,11 @@ __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
                     for (int fl = 0; fl < NFL; fl++) {
                         constexpr int SJ = (LK + 1) * (LL + 1), SI = (LJ + 1) * SJ;
                         const int ix = cart_pow(LI, fi, 0) * SI + cart_pow(LJ, fj, 0) * SJ +
-                                       cart_pow(LK, fk, 0) * (LL + 1) + cart_pow(LL, fl, 0);
+                                       cart_pow(LK, K0 + fk, 0) * (LL + 1) + cart_pow(LL, fl, 0);
                         const int iy = cart_pow(LI, fi, 1) * SI + cart_pow(LJ, fj, 1) * SJ +
-                                       cart_pow(LK, fk, 1) * (LL + 1) + cart_pow(LL, fl, 1);
+                                       cart_pow(LK, K0 + fk, 1) * (LL + 1) + cart_pow(LL, fl, 1);
                         const int iz = cart_pow(LI, fi, 2) * SI + cart_pow(LJ, fj, 2) * SJ +
-                                       cart_pow(LK, fk, 2) * (LL + 1) + cart_pow(LL, fl, 2);
+                                       cart_pow(LK, K0 + fk, 2) * (LL + 1) + cart_pow(LL, fl, 2);
                         acc[((fi * NFJ + fj) * NFK + fk) * NFL + fl] += g[0][ix] * g[1][iy] * g[2][iz];
                     }
                 }
@@ -303,7 +320,7 @@ __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
     // ---- digestion: one density block and one target at a time ----
     const int nao = A.nao;
     const size_t nn = (size_t)nao * nao;
-    const int i0t = __ldg(A.ao_loc + i_tile), k0t = __ldg(A.ao_loc + k_tile);
+    const int i0t = __ldg(A.ao_loc + i_tile), k0t = __ldg(A.ao_loc + k_tile) + K0;
 #define ACC(fi, fj, fk, fl) ((double)acc[(((fi) * NFJ + (fj)) * NFK + (fk)) * NFL + (fl)])
     for (int id = 0; id < A.n_dm; id++) {
         const double *__restrict__ D = A.dm + id * nn;
@@ -343,7 +360,7 @@ __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
             col_reduce<NKL, NRED>(pkl, s_red, [&](int cc, int n, double v) {
                 const int bb = b_begin + cc;
                 if (v != 0 && bb < b_end) {
-                    const int k0 = __ldg(A.ao_loc + __ldg(A.pair_bra + bb));
+                    const int k0 = __ldg(A.ao_loc + __ldg(A.pair_bra + bb)) + K0;
                     const int l0 = __ldg(A.ao_loc + __ldg(A.pair_ket + bb));
                     atomicAdd(VJ + (size_t)(k0 + n / NFL) * nao + l0 + n % NFL, v);
                 }
@@ -461,7 +478,7 @@ __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
                     col_reduce<NFI * NFK, NRED>(pik, s_red, [&](int cc, int n, double v) {
                         const int bb = b_begin + cc;
                         if (v != 0 && bb < b_end) {
-                            const int k0 = __ldg(A.ao_loc + __ldg(A.pair_bra + bb));
+                            const int k0 = __ldg(A.ao_loc + __ldg(A.pair_bra + bb)) + K0;
                             atomicAdd(VK + (size_t)(i0t + n / NFK) * nao + k0 + n % NFK, v);
                         }
                     });
@@ -794,6 +811,28 @@ static int launch_small(const JKArgs &args, const JKTask &task, int fp32, cudaSt
     return 0;
 }
 
+// Ket-split tile launches: jk_tile over fk in [K0, K0 + CK), [K0 + CK, ...)
+// until shell k is covered (one launch each).
+template <int LI, int LJ, int LK, int LL, typename F, int K0, int CK>
+static void launch_split_f(const JKArgs &args, const JKTask &task, int ntiles, cudaStream_t stream) {
+    constexpr int KN = imin(CK, ncart(LK) - K0);
+    jk_tile<LI, LJ, LK, LL, F, K0, KN><<<ntiles, 256, 0, stream>>>(args, task);
+    if constexpr (K0 + CK < ncart(LK))
+        launch_split_f<LI, LJ, LK, LL, F, K0 + CK, CK>(args, task, ntiles, stream);
+}
+
+template <int LI, int LJ, int LK, int LL, int CK>
+static int launch_split(const JKArgs &args, const JKTask &task, int fp32, cudaStream_t stream) {
+    int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
+    if (ntiles == 0) return 0;
+    bqc_count_launch(cdiv(ncart(LK), CK) - 1);   // the dispatcher counted one
+    if (fp32)
+        launch_split_f<LI, LJ, LK, LL, float, 0, CK>(args, task, ntiles, stream);
+    else
+        launch_split_f<LI, LJ, LK, LL, double, 0, CK>(args, task, ntiles, stream);
+    return 0;
+}
+
 template <int LI, int LJ, int LK, int LL, int NSPLIT, typename F>
 static int launch_group_f(const JKArgs &args, const JKTask &task, cudaStream_t stream) {
     using C = GroupCfg<LI, LJ, LK, LL, NSPLIT>;
@@ -821,22 +860,40 @@ static int launch_group(const JKArgs &args, const JKTask &task, int fp32, cudaSt
 // Small classes run one thread per quartet; larger ones put the pair with
 // fewer Cartesian components on the thread side and split the ket
 // components into chunks of at most ~36 accumulators.
+// Kernel choice per class (canonical order, bra pair index >= ket's):
+// at most SMALL_NF Cartesian components: jk_tile; otherwise, when shell k
+// splits into at most MAX_SPLIT ranges of fk whose blocks fit SMALL_NF,
+// ket-split jk_tile launches or jk_group as bqc_class_variant()
+// says (BQCset_class_variant; by default the split for classes of up to
+// SPLIT_AUTO ranges); else jk_group.
+constexpr int MAX_SPLIT = 3;
+constexpr int SPLIT_AUTO = 3;
+
 template <int L1, int L2, int L3, int L4>
 static int launch_class(const JKArgs &args, const JKTask &task, int fp32, cudaStream_t stream) {
     constexpr int N12 = ncart(L1) * ncart(L2), N34 = ncart(L3) * ncart(L4);
     if constexpr (N12 * N34 <= SMALL_NF) {
         return launch_small<L1, L2, L3, L4>(args, task, fp32, stream);
-    } else if constexpr (N12 <= N34) {
-        constexpr int NS = cdiv(N34, 36) > ncart(L3) ? ncart(L3) : cdiv(N34, 36);
-        return launch_group<L1, L2, L3, L4, NS>(args, task, fp32, stream);
     } else {
-        constexpr int NS = cdiv(N12, 36) > ncart(L1) ? ncart(L1) : cdiv(N12, 36);
-        JKTask sw = task;
-        sw.a0 = task.b0; sw.na = task.nb; sw.b0 = task.a0; sw.nb = task.na;
-        sw.pa0 = task.pb0; sw.pb0 = task.pa0; sw.nprim_a = task.nprim_b; sw.nprim_b = task.nprim_a;
-        sw.rows_are_b = !task.rows_are_b;
-        // diag tasks have identical lists on both sides; the a >= b rule stays
-        return launch_group<L3, L4, L1, L2, NS>(args, sw, fp32, stream);
+        constexpr int CK = SMALL_NF / (N12 * ncart(L4));
+        constexpr int NCH = CK >= 1 ? cdiv(ncart(L3), CK) : 0;
+        if constexpr (NCH >= 1 && NCH <= MAX_SPLIT) {
+            const int v = bqc_class_variant(L1, L2, L3, L4);
+            if (v == BQC_VARIANT_SPLIT || (v == BQC_VARIANT_AUTO && NCH <= SPLIT_AUTO))
+                return launch_split<L1, L2, L3, L4, CK>(args, task, fp32, stream);
+        }
+        if constexpr (N12 <= N34) {
+            constexpr int NS = cdiv(N34, 36) > ncart(L3) ? ncart(L3) : cdiv(N34, 36);
+            return launch_group<L1, L2, L3, L4, NS>(args, task, fp32, stream);
+        } else {
+            constexpr int NS = cdiv(N12, 36) > ncart(L1) ? ncart(L1) : cdiv(N12, 36);
+            JKTask sw = task;
+            sw.a0 = task.b0; sw.na = task.nb; sw.b0 = task.a0; sw.nb = task.na;
+            sw.pa0 = task.pb0; sw.pb0 = task.pa0; sw.nprim_a = task.nprim_b; sw.nprim_b = task.nprim_a;
+            sw.rows_are_b = !task.rows_are_b;
+            // diag tasks have identical lists on both sides; the a >= b rule stays
+            return launch_group<L3, L4, L1, L2, NS>(args, sw, fp32, stream);
+        }
     }
 }
 

@@ -18,7 +18,7 @@ SYMBOLS = ('GINTinit_basis_prod_cpu', 'GINTinit_basis_prod_gpu', 'GINTdel_basis_
            'GINTbuild_jk', 'BQCbuild_jk', 'BQCbuild_jk_mol', 'BQCbuild_jk_class', 'BQCcount_quartets',
            'BQCfp64_fma_peak', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e', 'BQClaunch_counter',
            'BQCbuild_jk_noalloc', 'BQCmlp_linear_fwd', 'BQCmlp_linear_bwd', 'BQCmlp_adam',
-           'BQCmlp_to_bf16', 'BQCversion')
+           'BQCmlp_to_bf16', 'BQCset_class_variant', 'BQCversion')
 
 
 def load_library(name='libbyteqc_b200'):

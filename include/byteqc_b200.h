@@ -189,6 +189,16 @@ int BQCmlp_adam(float *w, const float *g, float *m, float *v, void *w_bf16, int 
 /* y = bf16(x), n elements. */
 int BQCmlp_to_bf16(const float *x, void *y, size_t n, cudaStream_t stream);
 
+/* Kernel choice for shell-quartet class (li lj | lk ll) in this process, any
+ * order of the four: variant 0 = built-in rule, 1 = group kernel (threads
+ * per quartet share the 2D tables in shared memory), 2 = ket-split tile
+ * kernel (one thread per quartet, shell k's components in a few launches;
+ * only classes that split into at most 3 such launches, others ignore it).
+ * The choice changes speed only, never results.  Returns 0, 2 for l > 3,
+ * 3 for an unknown variant.  No reference counterpart (the reference has one
+ * fixed kernel per class, cuobc/lib/gvhf/nr_jk_driver.cu:40-225). */
+int BQCset_class_variant(int li, int lj, int lk, int ll, int variant);
+
 /* Number of kernel launches the library has issued in this process. */
 unsigned long long BQClaunch_counter(void);
 

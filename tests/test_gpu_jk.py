@@ -39,6 +39,31 @@ def test_jk_water(cuda, kind):
     assert abs(vk - rk).max() < TOL_JK * max(1, abs(rk).max() / 100)
 
 
+@pytest.mark.parametrize('variant', [1, 2])
+def test_jk_class_variants(cuda, variant):
+    """Every class in the group kernel (1) or, where it splits, in ket-split
+    tile launches (2): the same J/K as the oracle."""
+    from byteqc_b200 import lib as L
+    from byteqc_b200.scf import hf
+    lib = L.load_library()
+    shapes = [(a, b, c, d) for a in range(4) for b in range(a + 1)
+              for c in range(4) for d in range(c + 1)]
+    try:
+        for sh in shapes:
+            assert lib.BQCset_class_variant(*sh, variant) == 0
+        mol = _mol('cc-pvtz', nw=2, seed=4)
+        dm = _rand_dm(mol.nao) * 0.1
+        vj, vk = hf.get_jk(mol, dm)
+    finally:
+        for sh in shapes:
+            lib.BQCset_class_variant(*sh, 0)
+    rj, rk = oracle.get_jk(mol, dm)
+    assert abs(vj - rj).max() < 1e-9
+    assert abs(vk - rk).max() < 1e-9
+    assert lib.BQCset_class_variant(0, 0, 0, 0, 7) == 3
+    assert lib.BQCset_class_variant(4, 0, 0, 0, 1) == 2
+
+
 def test_jk_batch_and_flags(cuda):
     from byteqc_b200.scf import hf
     mol = _mol('cc-pvdz')
