@@ -526,10 +526,16 @@ struct GroupCfg {
     static constexpr int NG = imax(1, imin(256 / TPQ, SMEM_BUDGET / (PER_GROUP * 8)));
     static constexpr int NT = cdiv(NG * TPQ, 32) * 32;
     static constexpr size_t SMEM = (size_t)NG * PER_GROUP * sizeof(double);
+    // CTAs per SM the register budget is sized for: two when the shared
+    // memory lets two CTAs of at most 256 threads reside, else one (left to
+    // itself ptxas picks a budget that can be far too small for the large
+    // classes and spills heavily)
+    static constexpr int MINB = (NT <= 256 && 2 * (SMEM + 2048) <= 227 * 1024) ? 2 : 1;
 };
 
 template <int LI, int LJ, int LK, int LL, int NSPLIT, typename F>
-__global__ void __launch_bounds__(GroupCfg<LI, LJ, LK, LL, NSPLIT>::NT)
+__global__ void __launch_bounds__(GroupCfg<LI, LJ, LK, LL, NSPLIT>::NT,
+                                  GroupCfg<LI, LJ, LK, LL, NSPLIT>::MINB)
 jk_group(JKArgs A, JKTask T) {
     using C = GroupCfg<LI, LJ, LK, LL, NSPLIT>;
     constexpr int NFI = C::NFI, NFJ = C::NFJ, NFK = C::NFK, NFL = C::NFL;
