@@ -92,30 +92,6 @@ __device__ __forceinline__ void rys_roots(const double *__restrict__ table, doub
     }
 }
 
-// Order-1 rule from the Boys function: w = F0(x), s = F1(x) / F0(x).
-// x < 0.5: F1 = e^-x sum_k (2x)^k / (3 5 ... (2k+3)) and F0 = 2x F1 + e^-x;
-// otherwise F0 = sqrt(pi/x)/2 erf(sqrt x) and F1 = (F0 - e^-x) / (2x).
-__device__ __forceinline__ void rys_roots1(double x, double &s, double &w) {
-    double f0, f1;
-    if (x < 0.5) {
-        double e = exp(-x);
-        double term = 1.0 / 3.0, sum = term;
-#pragma unroll
-        for (int k = 1; k < 18; k++) {
-            term *= 2.0 * x / (2 * k + 3);
-            sum += term;
-        }
-        f1 = e * sum;
-        f0 = 2.0 * x * f1 + e;
-    } else {
-        double sx = sqrt(x);
-        f0 = 0.88622692545275801365 * erf(sx) / sx;
-        f1 = (f0 - exp(-x)) / (2.0 * x);
-    }
-    w = f0;
-    s = f1 / f0;
-}
-
 // One function of the order-N rule (q < N: node q, q >= N: weight q - N),
 // from the interval-major table (the lanes that call it for one x read the
 // same interval).

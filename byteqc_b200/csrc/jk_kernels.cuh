@@ -139,7 +139,7 @@ __device__ __forceinline__ void load_quartet(const JKArgs &A, int a, int b, Quar
 
 // primitive-pair quantities of one primitive quartet
 struct PrimQuartet {
-    double p, q, inv_pq, x, pref;
+    double p, q, inv_pq, inv_p, inv_q, x, pref;
     double PA[3], QC[3], PQ[3];
 };
 
@@ -151,8 +151,12 @@ __device__ __forceinline__ void load_prim(const JKArgs &A, const Quartet &Q, int
     double Qc[3] = {__ldg(A.x12 + pk), __ldg(A.y12 + pk), __ldg(A.z12 + pk)};
     P.p = aij;
     P.q = akl;
-    double s = aij + akl;
-    P.inv_pq = 1.0 / s;
+    const double s = aij + akl, pq = aij * akl;
+    // 1/(p+q), 1/p and 1/q from one division
+    const double t = 1.0 / (pq * s);
+    P.inv_pq = pq * t;
+    P.inv_p = akl * s * t;
+    P.inv_q = aij * s * t;
     double rr = 0;
 #pragma unroll
     for (int d = 0; d < 3; d++) {
@@ -161,8 +165,19 @@ __device__ __forceinline__ void load_prim(const JKArgs &A, const Quartet &Q, int
         P.PQ[d] = Pc[d] - Qc[d];
         rr += P.PQ[d] * P.PQ[d];
     }
-    P.x = aij * akl * P.inv_pq * rr;
-    P.pref = Q.fac * eij * ekl / (aij * akl * sqrt(s));
+    P.x = pq * P.inv_pq * rr;
+    P.pref = Q.fac * eij * ekl * (P.inv_p * P.inv_q) * rsqrt(s);
+}
+
+// recursion coefficients of root s, without a division
+__device__ __forceinline__ RootCoef root_coef(double s, const PrimQuartet &P) {
+    RootCoef c;
+    c.b00 = 0.5 * s * P.inv_pq;
+    c.qs = P.q * s * P.inv_pq;
+    c.ps = P.p * s * P.inv_pq;
+    c.b10 = 0.5 * (1.0 - c.qs) * P.inv_p;
+    c.b01 = 0.5 * (1.0 - c.ps) * P.inv_q;
+    return c;
 }
 
 // ---------------------------------------------------------------------------
@@ -282,11 +297,10 @@ __global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
                 PrimQuartet P;
                 load_prim(A, Q, pa + ip, pb + kp, P);
                 double rt[NR], wt[NR];
-                if constexpr (NR == 1) rys_roots1(P.x, rt[0], wt[0]);
-                else rys_roots<NR>(A.rys_lm, P.x, rt, wt);
+                rys_roots<NR>(A.rys_lm, P.x, rt, wt);
 #pragma unroll
                 for (int rr = 0; rr < NR; rr++) {
-                    RootCoef cf = root_coef(rt[rr], P.p, P.q, P.inv_pq);
+                    RootCoef cf = root_coef(rt[rr], P);
                     F g[3][GSZ];
 #pragma unroll
                     for (int d = 0; d < 3; d++) {
@@ -604,7 +618,7 @@ jk_group(JKArgs A, JKTask T) {
                 if (active) {
                     for (int task = lane; task < 3 * NR; task += TPQ) {
                         int r = task / 3, d = task % 3;
-                        RootCoef c = root_coef(rw[r], P.p, P.q, P.inv_pq);
+                        RootCoef c = root_coef(rw[r], P);
                         double seed = (d == 2) ? rw[NR + r] * P.pref : 1.0;
                         // d is a runtime index, so P and AB/CD sit in local memory
                         // (L1): measured faster than selecting from registers,

@@ -109,6 +109,16 @@ def _make_s_index_offsets(log_q, nbins=10, cutoff=1e-12):
 PAIR_TILE = 16
 
 
+def _tiles_by_first_q(tb, tk, tq, dummy):
+    """Sort the pairs inside each tile by q descending, then the tiles by
+    their first (largest) q, stably."""
+    oi = np.argsort(-tq, axis=1, kind='stable')
+    rows = np.arange(len(tq))[:, None]
+    tb, tk, tq, dummy = tb[rows, oi], tk[rows, oi], tq[rows, oi], dummy[rows, oi]
+    ot = np.argsort(-tq[:, 0], kind='stable')
+    return tb[ot].ravel(), tk[ot].ravel(), tq[ot].ravel(), dummy[ot].ravel()
+
+
 def _tile_order(bra, ket, q, layout='q'):
     """Order the pairs of one class in tiles of PAIR_TILE pairs.
 
@@ -128,37 +138,29 @@ def _tile_order(bra, ket, q, layout='q'):
     In every layout q is descending within a tile and the first q of every
     tile is descending along the list, which keeps the tile pruning of
     BQCbuild_jk valid.  Returns (bra, ket, q, is_padding)."""
-    if layout == 'hybrid':
-        n = len(q)
-        if n == 0:
-            return bra, ket, q, np.zeros(0, bool)
-        o = np.lexsort((-q, bra))
-        b, k, qq = bra[o], ket[o], q[o]
-        starts = np.flatnonzero(np.r_[True, b[1:] != b[:-1]])
-        sizes = np.diff(np.r_[starts, n])
-        gid = np.repeat(np.arange(len(starts)), sizes)
-        rank = np.arange(n) - starts[gid]
-        full = rank < (sizes[gid] // PAIR_TILE) * PAIR_TILE
-        rest = np.flatnonzero(~full)
-        rest = rest[np.argsort(-qq[rest], kind='stable')]
+    n = len(q)
+    if n == 0 and layout in ('q', 'hybrid'):
+        return bra, ket, q, np.zeros(0, bool)
+    if layout in ('q', 'hybrid'):
+        if layout == 'hybrid':
+            o = np.lexsort((-q, bra))
+            starts = np.flatnonzero(np.r_[True, bra[o][1:] != bra[o][:-1]])
+            sizes = np.diff(np.r_[starts, n])
+            gid = np.repeat(np.arange(len(starts)), sizes)
+            rank = np.arange(n) - starts[gid]
+            full = o[rank < (sizes[gid] // PAIR_TILE) * PAIR_TILE]
+            rest = o[rank >= (sizes[gid] // PAIR_TILE) * PAIR_TILE]
+        else:
+            full = np.zeros(0, np.int64)
+            rest = np.arange(n)
+        rest = rest[np.argsort(-q[rest], kind='stable')]
         pad = (-len(rest)) % PAIR_TILE
-        idx = np.r_[np.flatnonzero(full), rest, np.full(pad, rest[-1] if len(rest) else 0)]
-        tb, tk = b[idx].reshape(-1, PAIR_TILE), k[idx].reshape(-1, PAIR_TILE)
-        tq = np.r_[qq[idx[:n]], np.zeros(pad)].reshape(-1, PAIR_TILE)
-        ot = np.argsort(-tq[:, 0], kind='stable')
-        dummy = np.r_[np.zeros(n, bool), np.ones(pad, bool)].reshape(-1, PAIR_TILE)[ot]
-        return tb[ot].ravel(), tk[ot].ravel(), tq[ot].ravel(), dummy.ravel()
-    if layout == 'q':
-        n = len(q)
-        o = np.argsort(-q, kind='stable')
-        pad = (-n) % PAIR_TILE
-        if n == 0:
-            return bra, ket, q, np.zeros(0, bool)
-        out_b = np.r_[bra[o], np.repeat(bra[o[-1:]], pad)]
-        out_k = np.r_[ket[o], np.repeat(ket[o[-1:]], pad)]
-        out_q = np.r_[q[o], np.zeros(pad)]
-        dummy = np.r_[np.zeros(n, bool), np.ones(pad, bool)]
-        return out_b, out_k, out_q, dummy
+        idx = np.r_[full, rest, np.full(pad, rest[-1] if len(rest) else 0)].astype(np.int64)
+        tb = bra[idx].reshape(-1, PAIR_TILE)
+        tk = ket[idx].reshape(-1, PAIR_TILE)
+        tq = np.r_[q[idx[:n]], np.zeros(pad)].reshape(-1, PAIR_TILE)
+        dummy = np.r_[np.zeros(n, bool), np.ones(pad, bool)].reshape(-1, PAIR_TILE)
+        return _tiles_by_first_q(tb, tk, tq, dummy)
     if layout != 'shell':
         raise ValueError('unknown tile layout %r' % layout)
     n = len(q)
