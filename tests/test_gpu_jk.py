@@ -227,3 +227,25 @@ def test_mixed_precision_scf_energy(cuda):
     assert abs(e1 - e0) < 1e-9
     assert abs(e2 - e0) < 1e-9
     assert any(rec[1] > 0 for rec in mf1.build_log)
+
+
+def test_autotune_keeps_results(cuda):
+    """The autotuner picks kernels per class; J/K stay the same."""
+    import torch
+    from byteqc_b200 import autotune
+    from byteqc_b200 import lib as L
+    from byteqc_b200.scf import hf
+    mol = _mol('cc-pvtz', nw=2, seed=6)
+    opt = hf._VHFOpt(mol).build()
+    dm = torch.as_tensor(_rand_dm(mol.nao) * 0.1, device=cuda)[None]
+    vj0, vk0 = opt.jk_ao(dm)
+    try:
+        choice = autotune.tune(opt, reps=1)
+        assert choice and set(choice.values()) <= {1, 2}
+        vj1, vk1 = opt.jk_ao(dm)
+    finally:
+        lib = L.load_library()
+        for key in choice:
+            lib.BQCset_class_variant(*key, 0)
+    assert float((vj1 - vj0).abs().max()) < 1e-11
+    assert float((vk1 - vk0).abs().max()) < 1e-11

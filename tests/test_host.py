@@ -155,3 +155,15 @@ def test_tile_order_invariants(layout):
         if layout == 'shell' and n:
             Bt, Dt = B.reshape(-1, PAIR_TILE), D.reshape(-1, PAIR_TILE)
             assert np.all((Bt == Bt[:, :1]) | Dt)
+
+
+def test_autotune_variant_rule():
+    """The Python copy of the kernel-choice rule matches the classes that
+    have a ket-split variant (jk_kernels.cuh launch_class)."""
+    from byteqc_b200 import autotune
+    both = sorted({autotune.canonical(*c) for c in
+                   [(a, b, c, d) for a in range(4) for b in range(4) for c in range(4) for d in range(4)]
+                   if autotune.has_variants(*c)})
+    assert both == [(1, 1, 1, 1), (2, 1, 1, 1), (2, 1, 2, 0), (2, 2, 1, 0),
+                    (3, 0, 1, 1), (3, 0, 2, 0), (3, 0, 3, 0), (3, 1, 1, 0)]
+    assert autotune.canonical(0, 1, 2, 2) == (2, 2, 1, 0)
