@@ -237,8 +237,15 @@ __device__ __forceinline__ void col_reduce(double (&v)[NV], double (*s_red)[16][
 // k only (all of them by default).  Every J/K target is linear in the quartet
 // block, so launches over disjoint fk ranges add up to the whole class; a
 // class too large for one thread's registers runs as a few such launches.
+// CTAs per SM the register budget of jk_tile is sized for: small blocks
+// gain occupancy from a tighter budget, large ones need every register
+__host__ __device__ constexpr int tile_minb(int nf) {
+    return nf <= 3 ? 4 : (nf <= 9 ? 3 : (nf <= 27 ? 2 : 1));
+}
+
 template <int LI, int LJ, int LK, int LL, typename F, int K0 = 0, int KN = ncart(LK)>
-__global__ void __launch_bounds__(256) jk_tile(JKArgs A, JKTask T) {
+__global__ void __launch_bounds__(256, tile_minb(ncart(LI) * ncart(LJ) * KN * ncart(LL)))
+jk_tile(JKArgs A, JKTask T) {
     static_assert(K0 >= 0 && KN >= 1 && K0 + KN <= ncart(LK), "ket component range");
     // NFK: the components of shell k this launch evaluates, from K0 on
     constexpr int NFI = ncart(LI), NFJ = ncart(LJ), NFK = KN, NFL = ncart(LL);
