@@ -541,17 +541,21 @@ struct GroupCfg {
     static constexpr int DBUF = NIJ + NKL + NFI * NFK + NFI * NFL + NFJ * NFK + NFJ * NFL;
     static constexpr int RW = 2 * NR;
     static constexpr int PER_GROUP = RB + DBUF + RW;          // doubles
-    // groups per CTA: up to 256 threads and at most SMEM_BUDGET bytes of
-    // shared memory (two CTAs per SM)
-    static constexpr int SMEM_BUDGET = 112 * 1024;
-    static constexpr int NG = imax(1, imin(256 / TPQ, SMEM_BUDGET / (PER_GROUP * 8)));
+    // groups per CTA: up to NT_CAP threads and at most SMEM_BUDGET bytes of
+    // shared memory (four CTAs per SM; small CTAs let the barrier-separated
+    // phases of different CTAs overlap on an SM)
+    static constexpr int NT_CAP = 128;
+    static constexpr int SMEM_BUDGET = 56 * 1024;
+    static constexpr int NG = imax(1, imin(NT_CAP / TPQ, SMEM_BUDGET / (PER_GROUP * 8)));
     static constexpr int NT = cdiv(NG * TPQ, 32) * 32;
     static constexpr size_t SMEM = (size_t)NG * PER_GROUP * sizeof(double);
-    // CTAs per SM the register budget is sized for: two when the shared
-    // memory lets two CTAs of at most 256 threads reside, else one (left to
-    // itself ptxas picks a budget that can be far too small for the large
-    // classes and spills heavily)
-    static constexpr int MINB = (NT <= 256 && 2 * (SMEM + 2048) <= 227 * 1024) ? 2 : 1;
+    // CTAs per SM the register budget is sized for (128 registers a thread
+    // where the shared memory lets that many CTAs reside; left to itself
+    // ptxas picks a budget that can be far too small for the large classes
+    // and spills heavily)
+    static constexpr int MB_SMEM = (int)(227 * 1024 / (SMEM + 2048));
+    static constexpr int MB_THR = NT <= 128 ? 4 : (NT <= 256 ? 2 : 1);
+    static constexpr int MINB = imax(1, imin(MB_SMEM, MB_THR));
 };
 
 template <int LI, int LJ, int LK, int LL, int NSPLIT, typename F>
