@@ -182,7 +182,8 @@ def roofline(mf, peak):
             lk, ll, np_kl, _ = opt.cptype[ckl]
             f = nq * flops.quartet_flops(li, lj, lk, ll, np_ij, np_kl)
             rows.append({'class': '(%s%s|%s%s)' % tuple('spdf'[x] for x in (li, lj, lk, ll)),
-                         'nprim': [np_ij, np_kl], 'quartets': nq, 'ms': ms, 'flops': f})
+                         'nprim': [np_ij, np_kl], 'quartets': nq, 'ms': ms, 'flops': f,
+                         'prim_quartets': nq * np_ij * np_kl})
             total_t += ms
             total_f += f
     rows.sort(key=lambda r: -r['ms'])
@@ -197,7 +198,10 @@ def roofline(mf, peak):
         'peak_source': 'measured DFMA microbenchmark (BQCfp64_fma_peak) on this GPU',
         'build': {'ms': round(total_t, 2), 'tflops': round(total_f / (total_t * 1e-3) / 1e12, 3),
                   'frac': round(total_f / (total_t * 1e-3) / peak, 4),
-                  'quartets': int(sum(r['quartets'] for r in rows))},
+                  'quartets': int(sum(r['quartets'] for r in rows)),
+                  'quartets_per_s': float('%.4g' % (sum(r['quartets'] for r in rows) / (total_t * 1e-3))),
+                  'prim_quartets_per_s': float('%.4g' % (sum(r['prim_quartets'] for r in rows)
+                                                         / (total_t * 1e-3)))},
         'top_classes': [{k: (round(v, 3) if isinstance(v, float) else v) for k, v in r.items()}
                         for r in rows[:6]],
     }
