@@ -123,8 +123,9 @@ __device__ __forceinline__ double rys_one(const double *__restrict__ table, doub
 //   G(n+1, 0) = c00 G(n, 0) + n b10 G(n-1, 0)
 //   G(n, m+1) = c0p G(n, m) + m b01 G(n, m-1) + n b00 G(n-1, m)
 //   I(i, j+1) = I(i+1, j) + AB I(i, j)
-// The result g[i][j][k][l] is written to out[((i*(LJ+1)+j)*(LK+1)+k)*(LL+1)+l].
-template <int LI, int LJ, int LK, int LL, typename F>
+// The result g[i][j][k][l] is written to out[(i*(LJ+1)+j)*RS + k*(LL+1)+l]; the
+// row stride RS defaults to (LK+1)(LL+1) (dense) and can be padded.
+template <int LI, int LJ, int LK, int LL, typename F, int RS = (LK + 1) * (LL + 1)>
 __device__ __forceinline__ void gen_2d(F seed, F c00, F c0p, F b00, F b10, F b01, F ab, F cd,
                                        F *__restrict__ out) {
     constexpr int NM = LI + LJ + 1, MM = LK + LL + 1;
@@ -179,7 +180,7 @@ __device__ __forceinline__ void gen_2d(F seed, F c00, F c0p, F b00, F b10, F b01
             for (int k = 0; k <= LK; k++) {
 #pragma unroll
                 for (int l = 0; l <= LL; l++)
-                    out[((i * (LJ + 1) + j) * (LK + 1) + k) * (LL + 1) + l] = u[k][l];
+                    out[(i * (LJ + 1) + j) * RS + k * (LL + 1) + l] = u[k][l];
             }
         }
     }

@@ -109,6 +109,10 @@ __device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, in
     return count > 0;
 }
 
+__device__ __forceinline__ double sel3(const double (&v)[3], int d) {
+    return d == 0 ? v[0] : (d == 1 ? v[1] : v[2]);
+}
+
 struct Quartet {
     int a, b, ish, jsh, ksh, lsh, i0, j0, k0, l0;
     double A[3], B[3], C[3], D[3];
@@ -532,15 +536,20 @@ struct GroupCfg {
     static constexpr int TPQ = NIJ * NSPLIT;
     static constexpr int GSZ = (LI + 1) * (LJ + 1) * (LK + 1) * (LL + 1);
     static constexpr int KLS = (LK + 1) * (LL + 1);
+    // row stride of the 2D tables in shared memory, odd so that the rows
+    // the threads of a group read start in different banks
+    static constexpr int KLP = KLS | 1;
+    static constexpr int GSZP = (LI + 1) * (LJ + 1) * KLP;
     static constexpr int CK = cdiv(NFK, NSPLIT);
     static constexpr int NACC = CK * NFL;
-    static constexpr int GBUF = 3 * NR * GSZ;
+    static constexpr int GBUF = 3 * NR * GSZP;
     static constexpr int KSLOTS = 2 * NIJ * NFK + 2 * NIJ * NFL * NSPLIT;
     static constexpr int RB = imax(GBUF, KSLOTS);
     static constexpr int FKB = imax(1, RB / (NFL * NIJ));
     static constexpr int DBUF = NIJ + NKL + NFI * NFK + NFI * NFL + NFJ * NFK + NFJ * NFL;
     static constexpr int RW = 2 * NR;
-    static constexpr int PER_GROUP = RB + DBUF + RW;          // doubles
+    // doubles per group, odd so that neighbouring groups start in different banks
+    static constexpr int PER_GROUP = (RB + DBUF + RW) | 1;
     // groups per CTA: up to NT_CAP threads and at most SMEM_BUDGET bytes of
     // shared memory (four CTAs per SM; small CTAs let the barrier-separated
     // phases of different CTAs overlap on an SM)
@@ -592,9 +601,10 @@ jk_group(JKArgs A, JKTask T) {
 #pragma unroll
     for (int c = 0; c < NFJ; c++)
         if (c == fj) { pjx = cart_pow(LJ, c, 0); pjy = cart_pow(LJ, c, 1); pjz = cart_pow(LJ, c, 2); }
-    const int offx = (pix * (LJ + 1) + pjx) * C::KLS;
-    const int offy = GSZ * NR + (piy * (LJ + 1) + pjy) * C::KLS;
-    const int offz = 2 * GSZ * NR + (piz * (LJ + 1) + pjz) * C::KLS;
+    constexpr int GSZP = C::GSZP;
+    const int offx = (pix * (LJ + 1) + pjx) * C::KLP;
+    const int offy = GSZP * NR + (piy * (LJ + 1) + pjy) * C::KLP;
+    const int offz = 2 * GSZP * NR + (piz * (LJ + 1) + pjz) * C::KLP;
 
     const int nrounds = (count + NG - 1) / NG;
     for (int round = 0; round < nrounds; round++) {
@@ -631,22 +641,21 @@ jk_group(JKArgs A, JKTask T) {
                         int r = task / 3, d = task % 3;
                         RootCoef c = root_coef(rw[r], P);
                         double seed = (d == 2) ? rw[NR + r] * P.pref : 1.0;
-                        // d is a runtime index, so P and AB/CD sit in local memory
-                        // (L1): measured faster than selecting from registers,
-                        // which raises the register count of the whole kernel
-                        gen_2d<LI, LJ, LK, LL, F>(F(seed), F(P.PA[d] - c.qs * P.PQ[d]),
-                                                  F(P.QC[d] + c.ps * P.PQ[d]), F(c.b00), F(c.b10),
-                                                  F(c.b01), F(AB[d]), F(CD[d]),
-                                                  gtab + (d * NR + r) * GSZ);
+                        // d is a runtime index: select, so the arrays stay in registers
+                        const double pq = sel3(P.PQ, d);
+                        gen_2d<LI, LJ, LK, LL, F, C::KLP>(
+                            F(seed), F(sel3(P.PA, d) - c.qs * pq), F(sel3(P.QC, d) + c.ps * pq),
+                            F(c.b00), F(c.b10), F(c.b01), F(sel3(AB, d)), F(sel3(CD, d)),
+                            gtab + (d * NR + r) * GSZP);
                     }
                 }
                 __syncthreads();
                 if (active && lane < TPQ) {
 #pragma unroll
                     for (int r = 0; r < NR; r++) {
-                        const F *gx = gtab + offx + r * GSZ;
-                        const F *gy = gtab + offy + r * GSZ;
-                        const F *gz = gtab + offz + r * GSZ;
+                        const F *gx = gtab + offx + r * GSZP;
+                        const F *gy = gtab + offy + r * GSZP;
+                        const F *gz = gtab + offz + r * GSZP;
                         if constexpr (NSPLIT == 1) {
                             F xs[C::KLS], ys[C::KLS], zs[C::KLS];
 #pragma unroll
