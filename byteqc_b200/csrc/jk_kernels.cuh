@@ -641,11 +641,11 @@ jk_group(JKArgs A, JKTask T) {
                         int r = task / 3, d = task % 3;
                         RootCoef c = root_coef(rw[r], P);
                         double seed = (d == 2) ? rw[NR + r] * P.pref : 1.0;
-                        // d is a runtime index: select, so the arrays stay in registers
-                        const double pq = sel3(P.PQ, d);
+                        // d is a runtime index, so P and AB/CD sit in local memory
+                        // (L1): measured faster than selecting from registers
                         gen_2d<LI, LJ, LK, LL, F, C::KLP>(
-                            F(seed), F(sel3(P.PA, d) - c.qs * pq), F(sel3(P.QC, d) + c.ps * pq),
-                            F(c.b00), F(c.b10), F(c.b01), F(sel3(AB, d)), F(sel3(CD, d)),
+                            F(seed), F(P.PA[d] - c.qs * P.PQ[d]), F(P.QC[d] + c.ps * P.PQ[d]),
+                            F(c.b00), F(c.b10), F(c.b01), F(AB[d]), F(CD[d]),
                             gtab + (d * NR + r) * GSZP);
                     }
                 }
