@@ -24,7 +24,28 @@ struct JKArgs {
     int *status;              // device error word (0 = ok), may be NULL
     const double *rys;        // Rys coefficient table, interval-major (bqc_rys_table())
     const double *rys_lm;     // the same, level-major (bqc_rys_table_lm())
+    // ERI output mode (GINTfill_int2e) when eri != NULL: no density screen,
+    // no 1/2 for a == b, and instead of the J/K digestion every quartet adds
+    // its block (ij|kl) at eri[sum_n (ao_n - eri_off[n]) * eri_stride[n]]
+    double *eri;
+    long long eri_stride[4];
+    int eri_off[4];
 };
+
+// the same launch arguments with the bra and ket roles of the ERI output
+// exchanged (a kernel that evaluates (kl|ij) for (ij|kl))
+static inline JKArgs jk_args_swap_eri(const JKArgs &a) {
+    JKArgs s = a;
+    s.eri_stride[0] = a.eri_stride[2];
+    s.eri_stride[1] = a.eri_stride[3];
+    s.eri_stride[2] = a.eri_stride[0];
+    s.eri_stride[3] = a.eri_stride[1];
+    s.eri_off[0] = a.eri_off[2];
+    s.eri_off[1] = a.eri_off[3];
+    s.eri_off[2] = a.eri_off[0];
+    s.eri_off[3] = a.eri_off[1];
+    return s;
+}
 
 // One rectangular (or triangular, when diag) block of the quartet space.
 struct JKTask {

@@ -152,6 +152,7 @@ static JKArgs make_args(const BasisProdCache *bp, double *vj, double *vk, const 
     a.n_dm = n_dm;
     a.rys = bqc_rys_table();
     a.rys_lm = bqc_rys_table_lm();
+    a.eri = NULL;
     return a;
 }
 
@@ -181,6 +182,46 @@ int GINTbuild_jk(BasisProdCache *bpcache, double *vj, double *vk, double *dm, in
         t.nprim_b = ckl->nprim_12;
         t.diag = cp_ij_id == cp_kl_id;
         t.skip_lower = 1;
+        int err = bqc_launch_jk(cij->l_bra, cij->l_ket, ckl->l_bra, ckl->l_ket, args, t, 0, stream);
+        if (err) return err;
+    }
+    return 0;
+}
+
+// ERI writer (cuobc/lib/gint/nr_fill_ao_ints.cu:493-551): every quartet of the
+// class pair (cp_ij, cp_kl) whose bins satisfy ij_bin + kl_bin < nbins adds its
+// Cartesian block (ij|kl) to eri at sum_n (ao_n - ao_offsets[n]) strides[n];
+// all ij x kl pairs (no a >= b restriction, no 1/2 on identical pairs).
+int GINTfill_int2e(BasisProdCache *bpcache, double *eri, int nao, int *strides, int *ao_offsets,
+                   int *bins_locs_ij, int *bins_locs_kl, int nbins, int cp_ij_id, int cp_kl_id,
+                   cudaStream_t stream) {
+    if (eri == NULL || strides == NULL || ao_offsets == NULL) return 3;
+    if (cp_ij_id < 0 || cp_kl_id < 0 || cp_ij_id >= bpcache->ncptype || cp_kl_id >= bpcache->ncptype)
+        return 3;
+    const ContractionProdType *cij = bpcache->cptype + cp_ij_id;
+    const ContractionProdType *ckl = bpcache->cptype + cp_kl_id;
+    if (cij->l_bra > BQC_LMAX || ckl->l_bra > BQC_LMAX) return 2;
+    JKArgs args = make_args(bpcache, NULL, NULL, NULL, nao, 1);
+    args.eri = eri;
+    for (int n = 0; n < 4; n++) {
+        args.eri_stride[n] = strides[n];
+        args.eri_off[n] = ao_offsets[n];
+    }
+    for (int kl_bin = 0; kl_bin < nbins; kl_bin++) {
+        int kl0 = bins_locs_kl[kl_bin], kl1 = bins_locs_kl[kl_bin + 1];
+        if (kl1 <= kl0) continue;
+        int ij0 = bins_locs_ij[0], ij1 = bins_locs_ij[nbins - kl_bin];
+        if (ij1 <= ij0) continue;
+        JKTask t;
+        memset(&t, 0, sizeof(t));
+        t.a0 = bpcache->bas_pairs_locs[cp_ij_id] + ij0;
+        t.na = ij1 - ij0;
+        t.b0 = bpcache->bas_pairs_locs[cp_kl_id] + kl0;
+        t.nb = kl1 - kl0;
+        t.pa0 = bpcache->primitive_pairs_locs[cp_ij_id] + ij0 * cij->nprim_12;
+        t.pb0 = bpcache->primitive_pairs_locs[cp_kl_id] + kl0 * ckl->nprim_12;
+        t.nprim_a = cij->nprim_12;
+        t.nprim_b = ckl->nprim_12;
         int err = bqc_launch_jk(cij->l_bra, cij->l_ket, ckl->l_bra, ckl->l_ket, args, t, 0, stream);
         if (err) return err;
     }

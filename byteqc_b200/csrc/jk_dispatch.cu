@@ -45,7 +45,9 @@ int bqc_launch_jk(int li, int lj, int lk, int ll, const JKArgs &args, const JKTa
     // canonical order: pair index (l1*(l1+1)/2 + l2) of the bra >= that of the ket
     int pij = li * (li + 1) / 2 + lj, pkl = lk * (lk + 1) / 2 + ll;
     JKTask t = task;
+    JKArgs a_ = args;   // (not "a": the name is a parameter of BQC_CASE)
     if (pij < pkl) {
+        a_ = jk_args_swap_eri(args);
         std::swap(li, lk);
         std::swap(lj, ll);
         t.a0 = task.b0; t.na = task.nb; t.b0 = task.a0; t.nb = task.na;
@@ -58,7 +60,7 @@ int bqc_launch_jk(int li, int lj, int lk, int ll, const JKArgs &args, const JKTa
     int err = 0;
     switch (key) {
 #define BQC_CASE(a, b, c, d) \
-    case ((a * 4 + b) * 4 + c) * 4 + d: err = bqc_class_##a##b##c##d(args, t, fp32, stream); break;
+    case ((a * 4 + b) * 4 + c) * 4 + d: err = bqc_class_##a##b##c##d(a_, t, fp32, stream); break;
 #include "jk_classes.inc"
 #undef BQC_CASE
     default:

@@ -138,7 +138,7 @@ __device__ __forceinline__ void load_quartet(const JKArgs &A, int a, int b, Quar
         dst[s][1] = __ldg(A.bas_y + sh[s]);
         dst[s][2] = __ldg(A.bas_z + sh[s]);
     }
-    q.fac = (a == b) ? 0.5 * TWO_PI_2P5 : TWO_PI_2P5;
+    q.fac = (a == b && A.eri == nullptr) ? 0.5 * TWO_PI_2P5 : TWO_PI_2P5;
 }
 
 // primitive-pair quantities of one primitive quartet
@@ -340,6 +340,27 @@ jk_tile(JKArgs A, JKTask T) {
                 }
             }
         }
+    }
+
+    if (A.eri != nullptr) {
+        // ERI output mode: add the block, no digestion
+        if (active) {
+            const long long s0 = A.eri_stride[0], s1 = A.eri_stride[1], s2 = A.eri_stride[2],
+                            s3 = A.eri_stride[3];
+            double *base = A.eri + (Q.i0 - A.eri_off[0]) * s0 + (Q.j0 - A.eri_off[1]) * s1 +
+                           (Q.k0 - A.eri_off[2]) * s2 + (Q.l0 - A.eri_off[3]) * s3;
+#pragma unroll
+            for (int fi = 0; fi < NFI; fi++)
+#pragma unroll
+                for (int fj = 0; fj < NFJ; fj++)
+#pragma unroll
+                    for (int fk = 0; fk < NFK; fk++)
+#pragma unroll
+                        for (int fl = 0; fl < NFL; fl++)
+                            atomicAdd(base + fi * s0 + fj * s1 + fk * s2 + fl * s3,
+                                      (double)acc[((fi * NFJ + fj) * NFK + fk) * NFL + fl]);
+        }
+        return;
     }
 
     // ---- digestion: one density block and one target at a time ----
@@ -699,6 +720,27 @@ jk_group(JKArgs A, JKTask T) {
             }
         }
 
+        if (A.eri != nullptr) {
+            // ERI output mode: add this thread's components, no digestion
+            if (active && lane < TPQ) {
+                const long long s0 = A.eri_stride[0], s1 = A.eri_stride[1], s2 = A.eri_stride[2],
+                                s3 = A.eri_stride[3];
+                double *base = A.eri + (Q.i0 + fi - A.eri_off[0]) * s0 +
+                               (Q.j0 + fj - A.eri_off[1]) * s1 + (Q.k0 - A.eri_off[2]) * s2 +
+                               (Q.l0 - A.eri_off[3]) * s3;
+#pragma unroll
+                for (int ck = 0; ck < CK; ck++) {
+                    const int fk = chunk * CK + ck;
+                    if (fk < NFK) {
+#pragma unroll
+                        for (int fl = 0; fl < NFL; fl++)
+                            atomicAdd(base + fk * s2 + fl * s3, (double)acc[ck * NFL + fl]);
+                    }
+                }
+            }
+            continue;
+        }
+
         // ---- digestion ----
         const int nao = A.nao;
         const size_t nn = (size_t)nao * nao;
@@ -932,7 +974,7 @@ static int launch_class(const JKArgs &args, const JKTask &task, int fp32, cudaSt
             sw.pa0 = task.pb0; sw.pb0 = task.pa0; sw.nprim_a = task.nprim_b; sw.nprim_b = task.nprim_a;
             sw.rows_are_b = !task.rows_are_b;
             // diag tasks have identical lists on both sides; the a >= b rule stays
-            return launch_group<L3, L4, L1, L2, NS>(args, sw, fp32, stream);
+            return launch_group<L3, L4, L1, L2, NS>(jk_args_swap_eri(args), sw, fp32, stream);
         }
     }
 }

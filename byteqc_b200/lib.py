@@ -15,7 +15,7 @@ _lib = None
 
 # exported symbols, as declared in include/byteqc_b200.h
 SYMBOLS = ('GINTinit_basis_prod_cpu', 'GINTinit_basis_prod_gpu', 'GINTdel_basis_prod',
-           'GINTbuild_jk', 'BQCbuild_jk', 'BQCbuild_jk_mol', 'BQCbuild_jk_class', 'BQCcount_quartets',
+           'GINTbuild_jk', 'GINTfill_int2e', 'BQCbuild_jk', 'BQCbuild_jk_mol', 'BQCbuild_jk_class', 'BQCcount_quartets',
            'BQCfp64_fma_peak', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e', 'BQClaunch_counter',
            'BQCbuild_jk_noalloc', 'BQCmlp_linear_fwd', 'BQCmlp_linear_bwd', 'BQCmlp_adam',
            'BQCmlp_to_bf16', 'BQCset_class_variant', 'BQCversion')

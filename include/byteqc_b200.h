@@ -122,6 +122,19 @@ int BQCbuild_jk_class(const BasisProdCache *bpcache, int cp_ij, int cp_kl, const
                       double *vj, double *vk, const double *dm, int nao, int n_dm, double tol,
                       double fp32_below, int *status_dev, cudaStream_t stream);
 
+/* ERI writer, cuobc/lib/gint/nr_fill_ao_ints.cu:493-551 (GINTfill_int2e):
+ * every quartet of class pair (cp_ij_id, cp_kl_id) in the bins
+ * ij_bin + kl_bin < nbins (bins_locs_*: host, nbins + 1 offsets into the
+ * class's pair list) adds its Cartesian block (ij|kl), i and j from the bra
+ * pair, to eri[sum_n (ao_n - ao_offsets[n]) * strides[n]] (strides and
+ * ao_offsets: host, 4 entries for i, j, k, l).  No density screening, no
+ * symmetry: the caller fills the other index orders (cuobc/lib/int4c.py).
+ * The cache should be built with diag factor 1 for plain integrals.
+ * Returns 0, 1 on a CUDA error, 2 for l > 3, 3 for bad arguments. */
+int GINTfill_int2e(BasisProdCache *bpcache, double *eri, int nao, int *strides, int *ao_offsets,
+                   int *bins_locs_ij, int *bins_locs_kl, int nbins, int cp_ij_id, int cp_kl_id,
+                   cudaStream_t stream);
+
 /* Number of quartets of class pair (cp_ij, cp_kl) (all class pairs when
  * cp_ij < 0) that pass the screening of BQCbuild_jk, added to the device
  * counter *count_dev; no integrals are evaluated. */
