@@ -109,10 +109,6 @@ __device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, in
     return count > 0;
 }
 
-__device__ __forceinline__ double sel3(const double (&v)[3], int d) {
-    return d == 0 ? v[0] : (d == 1 ? v[1] : v[2]);
-}
-
 struct Quartet {
     int a, b, ish, jsh, ksh, lsh, i0, j0, k0, l0;
     double A[3], B[3], C[3], D[3];
@@ -613,8 +609,6 @@ jk_group(JKArgs A, JKTask T) {
 
     const int fij = lane / NSPLIT, chunk = lane % NSPLIT;
     const int fi = fij / NFJ, fj = fij % NFJ;
-    const int ixb = cart_pow(LI, 0, 0);  // silence unused warnings of constexpr helpers
-    (void)ixb;
     int pix = 0, piy = 0, piz = 0, pjx = 0, pjy = 0, pjz = 0;
 #pragma unroll
     for (int c = 0; c < NFI; c++)
