@@ -368,9 +368,7 @@ def main():
     launches = lib.BQClaunch_counter() - launches0
     t_step = float(np.mean(times))
     if world > 1:
-        tt = torch.tensor([t_step], device='cuda')
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        t_step = float(tt.item())
+        t_step = max_over_ranks(t_step, 'cuda')
         torch.distributed.barrier()
 
     line = {'metric': METRIC, 'value': round(t_step, 3), 'unit': 's', 'n_gpus': args.gpus,
@@ -439,6 +437,18 @@ def main():
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def max_over_ranks(value, device):
+    """The largest value over the ranks of the default process group: the
+    step time of N replicas is that of the slowest."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return value
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
 
 
 JKPY_DENSITY = 'random symmetric AO density (rand + rand^T) x 0.1, seed 2341'
