@@ -1,20 +1,26 @@
 """Benchmark of the direct-SCF J/K engine on one B200 (N GPUs: replicas).
 
-Workload (one step): a complete plain-FP64 RHF solve of (H2O)_64 in the
-cc-pVTZ-shaped synthetic basis (3712 AO, s-f shells) from a SAD guess to
-|Delta E| <= 1e-8 Eh, direct SCF with incremental Fock builds, Schwarz
-threshold 1e-13.  ``value`` is SCF wall seconds per solve (device time with
-CUDA events, setup included); ``e2e`` repeats the solve through the drop-in
-host API (a host SCF loop calling get_jk with numpy arrays every cycle, the
-way cuobc's RHF runs under pyscf).  The roofline object describes the
-dominant J/K kernel class of one full J+K build with the converged density.
+Workload (one step): a complete RHF solve of (H2O)_64 in the cc-pVTZ-shaped
+synthetic basis (3712 AO, s-f shells) from a SAD guess to |Delta E| <= 1e-8 Eh,
+direct SCF with incremental Fock builds, Schwarz threshold 1e-13, in the fast
+form (FP32 band and early screen on the builds before one full FP64 rebuild).
+``value`` is SCF wall seconds per solve (CUDA events, set-up included);
+``plain_fp64`` is the plain FP64 form on the same GPU; ``e2e`` repeats the
+fast solve through the drop-in host API (a host SCF loop calling get_jk with
+numpy arrays every cycle, the way cuobc's RHF runs under pyscf).  The
+roofline object describes the dominant J/K class pair and the whole build of
+one full J+K build with the converged density; the FLOP count of the plain
+solve is counted on the device in the same run.  ``cpu_baseline`` is the CPU
+oracle (an OpenMP C restatement of the reference's algorithm) timed on a
+complete SCF of (H2O)_4 in the cc-pVDZ shape on the host cores.
 
---impl reference: the CPU oracle (OpenMP C restatement of the reference's
-get_jk path) on the host cores, on a bounded sample of the same workload,
-projected to the workload by the algorithmic FLOP count; beside it
-(``reference_gpu``) one J/K build of the workload by the reference's own GPU
-kernels (oracle/_ref) on the same GPU, which the main line's ``jk_build``
-repeats with this engine on the same density.
+--impl reference: the same SCF along the reference's own path -- its J/K
+kernels (oracle/_ref: cuobc/lib/gint and gvhf compiled for sm_100a), its host
+logic (oracle/ref_gpu.py, oracle/ref_scf.py: Schwarz pair lists, class-level
+density screen, log-q bins, one GINTbuild_jk per class pair) and a pyscf-style
+host SCF loop -- on the same GPU.  One step of this arm is one SCF cycle;
+``value`` is the measured wall time of the complete SCF (set-up included)
+that the timed steps contain.  Nothing of the engine library is loaded.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -44,7 +50,6 @@ def parse():
     p.add_argument('--basis', default='cc-pvtz')
     p.add_argument('--conv', type=float, default=1e-8)
     p.add_argument('--no-extras', action='store_true', help='skip e2e/roofline/cpu legs')
-    p.add_argument('--account', action='store_true', help='recount the plain-SCF FLOPs')
     return p.parse_args()
 
 
@@ -192,7 +197,7 @@ def roofline(mf, peak):
     return {
         'bound': 'fp64', 'unit': 'TFLOP/s', 'achieved': round(achieved, 3),
         'peak': round(peak / 1e12, 3), 'frac': round(achieved * 1e12 / peak, 4),
-        'traffic': None,
+        'traffic': TRAFFIC.get(top['class']),
         'kernel': 'J/K class pair %s nprim %s (%.1f%% of the build)' % (
             top['class'], top['nprim'], 100 * top['ms'] / total_t),
         'peak_source': 'measured DFMA microbenchmark (BQCfp64_fma_peak) on this GPU',
@@ -240,54 +245,26 @@ def jk_flops(opt, dm_ao):
     return tot
 
 
-def scf_flops(mol, conv):
-    """Algorithmic FLOPs of the J/K builds of one plain-FP64 SCF solve."""
-    import torch
-    from byteqc_b200.scf import hf, guess
-    guess._SAD_CACHE.clear()
-    mf = hf.RHF(mol)
-    mf.conv_tol = conv
-    acc = []
-    mf.jk_hook = lambda d, fp32_below: acc.append(jk_flops(mf.opt, d))
-    mf.kernel()
-    return float(sum(acc)), len(acc)
-
-
-def cpu_sample(args, threads):
-    """Oracle J/K build of a bounded sample; returns (seconds, flops of the
-    sample under the FLOP convention, description)."""
+def cpu_oracle_scf(threads):
+    """The CPU oracle on a bounded sample: a complete RHF of (H2O)_4 in the
+    cc-pVDZ shape (96 AO) to |Delta E| < 1e-8 with exact J/K (no screening)
+    on `threads` host threads.  Returns (seconds, energy, cycles, sample)."""
     from byteqc_b200.gto.mole import Mole
     from byteqc_b200.gto.basis import synthetic_basis
     from byteqc_b200.gto.geom import water_cluster
     from oracle import oracle
-    nw = 2
-    mol = Mole(water_cluster(nw, seed=0), synthetic_basis(args.basis, ['O', 'H']))
-    rng = np.random.default_rng(2341)
-    dm = rng.random((mol.nao, mol.nao))
-    dm = dm + dm.T
+    mol = Mole(water_cluster(4, seed=0), synthetic_basis('cc-pvdz', ['O', 'H']))
     t0 = time.perf_counter()
-    oracle.get_jk(mol, dm, nthreads=threads)
+    e, _, cycles = oracle.rhf(mol, conv_tol=1e-8, nthreads=threads)
     t = time.perf_counter() - t0
-    return t, mol, '(H2O)%d/%s-shaped, one exact J+K build (no screening), %d threads' % (
-        nw, args.basis, threads)
+    return t, e, cycles, ('(H2O)4/cc-pvdz-shaped (96 AO, seed 0): one complete RHF to |dE| < 1e-8 '
+                          'from the core guess, exact J/K every cycle, %d threads; %d cycles' % (
+                              threads, cycles))
 
 
-def oracle_flops(mol):
-    """Algorithmic FLOPs of the oracle's exact build (every unique quartet of
-    the contracted basis, general contractions counted per column)."""
-    from byteqc_b200 import flops
-    ls = mol._bas[:, 1]
-    npr = mol._bas[:, 2]
-    nc = mol._bas[:, 3]
-    nb = mol.nbas
-    tot = 0.
-    pairs = [(i, j) for i in range(nb) for j in range(i + 1)]
-    for a, (i, j) in enumerate(pairs):
-        for b in range(a + 1):
-            k, l = pairs[b]
-            c = nc[i] * nc[j] * nc[k] * nc[l]
-            tot += c * flops.quartet_flops(ls[i], ls[j], ls[k], ls[l], npr[i] * npr[j], npr[k] * npr[l])
-    return tot
+# DRAM bytes per launch of the J/K kernels (dram__bytes_read.sum +
+# dram__bytes_write.sum of one ncu capture), by class; see profiles/.
+TRAFFIC = {}
 
 
 def main():
@@ -297,43 +274,8 @@ def main():
     local = int(os.environ.get('LOCAL_RANK', 0))
 
     if args.impl == 'reference':
-        if rank != 0:
-            return
-        threads = os.cpu_count() or 1
-        mol_full = workload(args)
-        for _ in range(args.warmup):
-            cpu_sample(args, threads)
-        ts = []
-        for _ in range(args.steps):
-            t_s, mol_s, desc = cpu_sample(args, threads)
-            ts.append(t_s)
-        t_s = float(np.mean(ts))
-        f_s = oracle_flops(mol_s)
-        rate = f_s / t_s
-        # project the plain-FP64 SCF of the workload: the FLOPs that the GPU
-        # solve needs (same convention) at the oracle's measured rate
-        key = '(H2O)%d/%s' % (args.nwater, args.basis)
-        recs = json.load(open(os.path.join(ROOT, 'bench_workload_flops.json')))['workloads']
-        if key not in recs:
-            print(json.dumps({'impl': 'reference', 'unavailable': 'no recorded FLOP count for %s' % key}))
-            return
-        ref = recs[key]
-        value = ref['scf_flops'] / rate
-        line = {'impl': 'reference', 'metric': METRIC, 'value': round(value, 2), 'unit': 's',
-                'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
-                'higher_is_better': False, 'dtype': 'f64', 'data': 'synthetic',
-                'config': config(args, mol_full),
-                'cpu_baseline': {'value': round(value, 2), 'unit': 's', 'cores': threads,
-                                 'kind': 'port', 'sample': desc + '; %.3g FLOP in %.2f s, projected '
-                                 'to the %.3g FLOP of the workload SCF' % (f_s, t_s, ref['scf_flops'])},
-                'e2e': {'value': round(value, 2), 'unit': 's', 'h2d_bytes_per_step': 0,
-                        'd2h_bytes_per_step': 0}}
-        # the reference's own GPU kernels on the same GPU, one J/K build
-        try:
-            line['reference_gpu'] = reference_gpu_build(mol_full)
-        except Exception as exc:   # report, never fail the CPU line
-            line['reference_gpu'] = {'unavailable': '%s: %s' % (type(exc).__name__, exc)}
-        print(json.dumps(line))
+        if rank == 0:
+            run_reference(args)
         return
 
     import torch
@@ -385,58 +327,212 @@ def main():
                     'jk_s': round(mf.timings.get('jk', 0), 3)}}
 
     if not args.no_extras and rank == 0:
-        # the plain FP64 form on the same GPU, same workload
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record()
-        mf_p, e_p = scf_once(mol, args.conv)
-        ev1.record()
-        torch.cuda.synchronize()
-        t_plain = ev0.elapsed_time(ev1) / 1e3
-        line['plain_fp64'] = {'value': round(t_plain, 3), 'unit': 's', 'cycles': mf_p.cycles,
-                              'energy': e_p, 'jk_s': round(mf_p.timings.get('jk', 0), 3),
-                              'speedup_fast_vs_plain': round(t_plain / t_step, 3),
-                              'energy_diff_fast_vs_plain': abs(e - e_p)}
-        # e2e through the drop-in host API
-        t0 = time.perf_counter()
-        mf_h, e_h = scf_once(mol, args.conv, host_loop=True, fast=True)
-        t_e2e = time.perf_counter() - t0
-        h2d, d2h = mf_h.host_bytes
-        line['e2e'] = {'value': round(t_e2e, 3), 'unit': 's', 'h2d_bytes_per_step': int(h2d),
-                       'd2h_bytes_per_step': int(d2h),
-                       'path': 'host SCF loop calling get_jk(mol, dm_host) every cycle',
-                       'energy_diff_vs_device_loop': abs(e_h - e)}
-        peak = ctypes_peak(lib)
-        line['roofline'] = roofline(mf, peak)
-        # one J/K build on the density of the reference's timing script (the
-        # reference arm times its own kernels on the same one)
-        opt = mf.opt
-        dmc = jkpy_density(opt)
-        line['jk_build'] = {'s': round(time_build(lambda: opt.jk_cart(dmc)), 3),
-                            'density': JKPY_DENSITY, 'tol': opt.direct_scf_tol}
-        # FLOPs of the J/K builds of a plain-FP64 solve: the CPU projection's
-        # numerator (recorded per workload; --account recounts on the device)
-        key = '(H2O)%d/%s' % (args.nwater, args.basis)
-        recs = json.load(open(os.path.join(ROOT, 'bench_workload_flops.json')))['workloads']
-        if args.account or key not in recs:
-            f_scf, nbuild = scf_flops(mol, args.conv)
-            line['scf']['jk_builds_counted'] = nbuild
-        else:
-            f_scf = recs[key]['scf_flops']
-        line['scf']['plain_jk_flops'] = f_scf
-        line['scf']['plain_jk_tflops'] = round(f_scf / max(mf_p.timings.get('jk', 1e-9), 1e-9) / 1e12, 3)
-        ref = {'scf_flops': f_scf}
-        threads = os.cpu_count() or 1
-        t_s, mol_s, desc = cpu_sample(args, threads)
-        f_s = oracle_flops(mol_s)
-        cpu_val = ref['scf_flops'] / (f_s / t_s)
-        line['cpu_baseline'] = {'value': round(cpu_val, 2), 'unit': 's', 'cores': threads,
-                                'kind': 'port', 'sample': desc + '; %.3g FLOP in %.2f s, projected '
-                                'to the %.3g FLOP of the workload SCF' % (f_s, t_s, ref['scf_flops'])}
+        extras(args, mol, mf, e, t_step, line, lib)
     if rank == 0:
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def extras(args, mol, mf, e, t_step, line, lib):
+    """The legs beside the timed steps (rank 0): plain FP64 form, e2e through
+    the host API, roofline, J/K build on the reference's timing density with
+    the cross-check against the reference arm's output, FLOPs of the plain
+    solve counted on the device, and the CPU oracle baseline."""
+    import torch
+    # the plain FP64 form on the same GPU, same workload; its J/K input
+    # densities are kept for the FLOP count
+    from byteqc_b200.scf import hf, guess
+    guess._SAD_CACHE.clear()
+    mf_p = hf.RHF(mol)
+    mf_p.conv_tol = args.conv
+    dens = []
+    mf_p.jk_hook = lambda d, fp32_below: dens.append(d.clone())
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    e_p = mf_p.kernel()
+    ev1.record()
+    torch.cuda.synchronize()
+    t_plain = ev0.elapsed_time(ev1) / 1e3
+    line['plain_fp64'] = {'value': round(t_plain, 3), 'unit': 's', 'cycles': mf_p.cycles,
+                          'energy': e_p, 'jk_s': round(mf_p.timings.get('jk', 0), 3),
+                          'speedup_fast_vs_plain': round(t_plain / t_step, 3),
+                          'energy_diff_fast_vs_plain': abs(e - e_p)}
+    # e2e through the drop-in host API
+    t0 = time.perf_counter()
+    mf_h, e_h = scf_once(mol, args.conv, host_loop=True, fast=True)
+    t_e2e = time.perf_counter() - t0
+    h2d, d2h = mf_h.host_bytes
+    line['e2e'] = {'value': round(t_e2e, 3), 'unit': 's', 'h2d_bytes_per_step': int(h2d),
+                   'd2h_bytes_per_step': int(d2h),
+                   'path': 'host SCF loop calling get_jk(mol, dm_host) every cycle',
+                   'energy_diff_vs_device_loop': abs(e_h - e)}
+    peak = ctypes_peak(lib)
+    line['roofline'] = roofline(mf, peak)
+    # FLOPs of the plain solve's J/K builds, counted on its own densities
+    f_scf = sum(jk_flops(mf_p.opt, d) for d in dens)
+    del dens
+    line['scf']['plain_jk_flops'] = f_scf
+    line['scf']['plain_jk_builds'] = mf_p.cycles
+    line['scf']['plain_jk_tflops'] = round(f_scf / max(mf_p.timings.get('jk', 1e-9), 1e-9) / 1e12, 3)
+    line['scf']['plain_jk_frac_of_fp64_peak'] = round(
+        f_scf / max(mf_p.timings.get('jk', 1e-9), 1e-9) / peak, 4)
+    # one J/K build on the density of the reference's timing script; the
+    # reference arm (run first by the driver) leaves its J/K and SCF energy
+    opt = mf.opt
+    dmc = jkpy_density(opt)
+    line['jk_build'] = {'s': round(time_build(lambda: opt.jk_cart(dmc)), 3),
+                        'density': JKPY_DENSITY, 'tol': opt.direct_scf_tol}
+    line['jk_build']['reference_check'] = reference_check(args, opt, dmc, e_p)
+    # CPU baseline: the oracle on a bounded sample, host cores
+    threads = os.cpu_count() or 1
+    t_cpu, e_cpu, cyc, desc = cpu_oracle_scf(threads)
+    line['cpu_baseline'] = {'value': round(t_cpu, 2), 'unit': 's', 'cores': threads,
+                            'kind': 'port', 'sample': desc}
+    # the same sample on this engine, for a like-for-like ratio
+    from byteqc_b200.gto.mole import Mole
+    from byteqc_b200.gto.basis import synthetic_basis
+    from byteqc_b200.gto.geom import water_cluster
+    small = Mole(water_cluster(4, seed=0), synthetic_basis('cc-pvdz', ['O', 'H']))
+
+    def small_scf():
+        m = hf.RHF(small)
+        m.conv_tol = 1e-8
+        m.init_guess = '1e'
+        return m.kernel()
+    small_scf()
+    ev0.record()
+    e_s = small_scf()
+    ev1.record()
+    torch.cuda.synchronize()
+    line['cpu_baseline']['same_sample_on_gpu_s'] = round(ev0.elapsed_time(ev1) / 1e3, 3)
+    line['cpu_baseline']['energy_diff_gpu_vs_oracle'] = abs(e_s - e_cpu)
+
+
+REF_OUT = os.path.join(os.environ.get('TMPDIR', '/tmp'), 'byteqc_b200_reference_%s.npz')
+
+
+def _ref_key(args):
+    return '%dw_%s' % (args.nwater, args.basis.replace('*', 's'))
+
+
+def reference_check(args, opt, dmc, e_plain):
+    """J/K of the timing density and the SCF energy against what the
+    reference arm computed on the same workload (its file, when present):
+    max |dJ|, max |dK| in the AO basis and |dE|.  The two builds screen
+    differently (per quartet here, per class pair and log-q bin there), so
+    they differ by at most what either screen drops."""
+    path = REF_OUT % _ref_key(args)
+    if not os.path.exists(path):
+        return {'skipped': 'the reference arm has not run on this box'}
+    import torch
+    ref = np.load(path)
+    J, K = opt.jk_cart(dmc)
+    C = opt.coeff_dev
+    J = (C.T @ J[0] @ C).cpu().numpy()
+    K = (C.T @ K[0] @ C).cpu().numpy()
+    dj = float(abs(J - ref['J']).max())
+    dk = float(abs(K - ref['K']).max())
+    out = {'max_abs_dJ': dj, 'max_abs_dK': dk, 'max_abs_J': float(abs(ref['J']).max()),
+           'bound': SCREEN_BOUND, 'within_bound': dj < SCREEN_BOUND and dk < SCREEN_BOUND}
+    if 'energy' in ref.files:
+        out['scf_energy_diff_vs_reference'] = abs(float(ref['energy']) - e_plain)
+    return out
+
+
+# Bound on the difference of two J/K builds that both drop only quartets
+# whose estimate q_ij q_kl max|D| is below 1e-13: a J or K element collects at
+# most ~1e4 such dropped contributions at this size.
+SCREEN_BOUND = 1e-8
+
+
+def run_reference(args):
+    """The reference arm: the reference's SCF path with its own GPU kernels
+    (see the module doc).  Steps are SCF cycles: W untimed cycles of the
+    workload's SCF, then a fresh SCF (set-up included) timed to convergence,
+    followed by repeats of its last cycle until K steps are done."""
+    import torch
+    from oracle import ref_gpu
+    base = {'impl': 'reference', 'metric': METRIC}
+    if not torch.cuda.is_available():
+        print(json.dumps(dict(base, unavailable='no CUDA device')))
+        return
+    if not ref_gpu.available():
+        print(json.dumps(dict(base, unavailable='oracle/_ref not built: the reference sources '
+                                                'were absent when the package was built')))
+        return
+    from oracle.ref_scf import RefSCF
+    torch.cuda.set_device(0)
+    mol = workload(args)
+    threads = os.cpu_count() or 1
+    if args.warmup > 0:
+        warm = RefSCF(mol, conv_tol=args.conv, max_cycle=args.warmup)
+        warm.kernel()
+        warm.close()
+    torch.cuda.synchronize()
+    steps = 0
+    with ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        ref = RefSCF(mol, conv_tol=args.conv)
+        e = ref.kernel()
+        torch.cuda.synchronize()
+        t_scf = time.perf_counter() - t0
+        steps = ref.cycles
+        while steps < args.steps:
+            ref.repeat_cycle()
+            steps += 1
+        torch.cuda.synchronize()
+        t_all = time.perf_counter() - t0
+    nao0 = mol.nao
+    nao_c = ref.opt.coeff.shape[0]
+    # host <-> device bytes of one cycle along the reference path: D in, D' back
+    # for the class screen, J and K back; F and S in and C, e back for eig
+    h2d = 8 * (nao0 * nao0 + 2 * nao0 * nao0)
+    d2h = 8 * (nao_c * nao_c + 2 * nao0 * nao0 + nao0 * nao0 + nao0)
+    line = dict(base, **{
+        'value': round(t_scf, 3), 'unit': 's', 'n_gpus': args.gpus, 'steps': steps,
+        'warmup': args.warmup, 'ms_per_step': round(t_all / steps * 1e3, 1),
+        'higher_is_better': False, 'dtype': 'f64', 'data': 'synthetic',
+        'config': config(args, mol), 'clocks': clk.summary(),
+        'step': 'one SCF cycle of the reference path; value = wall seconds of the complete '
+                'SCF (set-up, Schwarz pair lists, guess, %d cycles to |dE| < %g) inside the '
+                'timed steps' % (ref.cycles, args.conv),
+        'cpu_baseline': {'value': round(t_scf, 3), 'unit': 's', 'cores': threads,
+                         'kind': 'reference',
+                         'sample': 'the complete workload SCF: the reference J/K kernels '
+                                   '(oracle/_ref) on the GPU, host SCF loop on %d host '
+                                   'threads' % threads},
+        'e2e': {'value': round(t_scf, 3), 'unit': 's', 'h2d_bytes_per_step': h2d,
+                'd2h_bytes_per_step': d2h},
+        'scf': {'energy': e, 'cycles': ref.cycles, 'converged': bool(ref.converged),
+                'setup_s': round(ref.timings.get('setup', 0.), 3),
+                'pair_lists_s': round(ref.timings.get('vhfopt', 0.), 3),
+                'cycle_s': [round(x, 3) for x in ref.cycle_s]}})
+    # one J/K build on the density of the reference's timing script
+    # (cuobc/test/jk.py), timed; J, K and the SCF energy are left for the
+    # engine arm's cross-check
+    try:
+        rng = np.random.default_rng(2341)
+        dm = rng.random((nao0, nao0))
+        dm = 0.1 * (dm + dm.T)
+        C = ref.coeff
+        dmc = (C @ torch.as_tensor(dm, device='cuda') @ C.T)[None].contiguous()
+        tasks = ref.jk.tasks(dmc)
+        out = {}
+        t = time_build(lambda: out.setdefault('jk', ref.jk.jk_cart(dmc, tasks=tasks)), reps=1)
+        J, K = ref.jk.jk_cart(dmc, tasks=tasks)
+        np.savez(REF_OUT % _ref_key(args), J=(C.T @ J[0] @ C).cpu().numpy(),
+                 K=(C.T @ K[0] @ C).cpu().numpy(), energy=e)
+        line['reference_gpu'] = {
+            'jk_build_s': round(t, 3), 'density': JKPY_DENSITY, 'launches': len(tasks),
+            'what': 'GINTbuild_jk of the reference (cuobc/lib/gvhf, cuobc/lib/gint) built for '
+                    'sm_100a, driven by the restated host logic of cuobc/scf/hf.py get_jk '
+                    '(log-q bins, class-level density screen); same B200, CUDA events'}
+    except Exception as exc:   # report, never fail the line
+        line['reference_gpu'] = {'unavailable': '%s: %s' % (type(exc).__name__, exc)}
+    ref.close()
+    print(json.dumps(line))
 
 
 def max_over_ranks(value, device):
@@ -481,28 +577,6 @@ def time_build(fn, reps=2):
         torch.cuda.synchronize()
         best = min(best, e0.elapsed_time(e1) / 1e3)
     return best
-
-
-def reference_gpu_build(mol):
-    """Seconds of one J/K build by the reference's own GPU kernels (oracle/_ref,
-    compiled from cuobc/lib for sm_100a) on the jk.py density, or a reason."""
-    import torch
-    from oracle import ref_gpu
-    if not torch.cuda.is_available():
-        return {'unavailable': 'no GPU'}
-    if not ref_gpu.available():
-        return {'unavailable': 'oracle/_ref not built (the reference sources were absent at build time)'}
-    from byteqc_b200.scf import hf
-    opt = hf._VHFOpt(mol).build()
-    ref = ref_gpu.RefJK(opt)
-    dmc = jkpy_density(opt)
-    tasks = ref.tasks(dmc)
-    t = time_build(lambda: ref.jk_cart(dmc, tasks=tasks), reps=1)
-    ref.close()
-    return {'jk_build_s': round(t, 3), 'density': JKPY_DENSITY, 'launches': len(tasks),
-            'what': 'GINTbuild_jk of the reference (cuobc/lib/gvhf, cuobc/lib/gint) built for '
-                    'sm_100a, driven by the restated host logic of cuobc/scf/hf.py get_jk '
-                    '(log-q bins, class-level density screen); same B200, CUDA events'}
 
 
 def ctypes_peak(lib):

@@ -6,6 +6,7 @@ next to this file.  ``python -m byteqc_b200.build`` or ``build()``.
 """
 import concurrent.futures as cf
 import os
+import re
 import shutil
 import subprocess
 import sys
@@ -52,17 +53,31 @@ def _class_units():
     return units
 
 
-def _deps_mtime():
-    m = 0
-    for f in os.listdir(CSRC):
-        m = max(m, os.path.getmtime(os.path.join(CSRC, f)))
-    m = max(m, os.path.getmtime(os.path.join(INCLUDE, 'byteqc_b200.h')))
-    return m
+_INCLUDE_RE = re.compile(r'^\s*#\s*include\s+"([^"]+)"', re.M)
+
+
+def _deps(src, seen=None):
+    """The source file and every local header it includes, recursively
+    (looked up next to the including file, then in csrc/ and include/)."""
+    seen = set() if seen is None else seen
+    if src in seen:
+        return seen
+    seen.add(src)
+    with open(src) as f:
+        text = f.read()
+    for name in _INCLUDE_RE.findall(text):
+        for d in (os.path.dirname(src), CSRC, INCLUDE):
+            path = os.path.join(d, name)
+            if os.path.exists(path):
+                _deps(os.path.abspath(path), seen)
+                break
+    return seen
 
 
 def _compile(src, extra=()):
     obj = os.path.join(BUILD, os.path.basename(src).replace('.cu', '.o'))
-    if os.path.exists(obj) and os.path.getmtime(obj) > max(_deps_mtime(), os.path.getmtime(src)):
+    if os.path.exists(obj) and \
+            os.path.getmtime(obj) > max(os.path.getmtime(d) for d in _deps(os.path.abspath(src))):
         return obj
     cmd = [NVCC] + ARCH + FLAGS + list(extra) + ['-c', src, '-o', obj]
     t0 = time.time()

@@ -2,7 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
-#include "../../include/byteqc_b200.h"
+#include "byteqc_b200.h"
 
 #define BQC_LMAX 3          // s, p, d, f
 #define BQC_NCART_MAX 10

@@ -100,8 +100,11 @@ void GINTinit_basis_prod_gpu(BasisProdCache **pbpin, BasisProdCache **pbp, int *
     BasisProdCache *bp = (BasisProdCache *)malloc(sizeof(BasisProdCache));
     memcpy(bp, *pbpin, sizeof(BasisProdCache));
     *pbp = bp;
-    // the device copy shares the host class table; only the cpu cache owns it
-    bp->aexyz = NULL;
+    // The copy shares the host class table, primitive-pair offsets and host
+    // aexyz block with the cpu cache (the reference's ownership,
+    // cuobc/lib/gint/nr_fill_ao_ints.cu:472-491): GINTdel_basis_prod on
+    // either struct frees them, and cuobc/scf/hf.py:439-442 deletes only
+    // the device copy.
     bp->ao_loc = ao_loc;
     bp->bas_coords = bas_coords;
     int npairs = bp->bas_pairs_locs[bp->ncptype];
@@ -115,15 +118,19 @@ void GINTinit_basis_prod_gpu(BasisProdCache **pbpin, BasisProdCache **pbp, int *
     bp->bas_pair2ket = bas_pair2shls + npairs;
 }
 
+// Frees the struct and the host blocks it points at (class table,
+// primitive-pair offsets, host aexyz), as cuobc/lib/gint/nr_fill_ao_ints.cu:394-410
+// does.  A cpu cache and its device copies share those blocks: a caller that
+// keeps both deletes one of them, or clears the shared pointers of the other
+// first.
 void GINTdel_basis_prod(BasisProdCache **pbp) {
     BasisProdCache *bp = *pbp;
     if (bp == NULL) return;
-    if (bp->aexyz != NULL) {
-        // host cache: owns the class table and the primitive-pair block
+    if (bp->cptype != NULL) {
         free(bp->cptype);
         free(bp->primitive_pairs_locs);
-        free(bp->aexyz);
     }
+    if (bp->aexyz != NULL) free(bp->aexyz);
     free(bp);
     *pbp = NULL;
 }
@@ -490,6 +497,8 @@ int BQCbuild_jk_noalloc(const BasisProdCache *bp, const double *pair_q, double *
                 BQC_NOALLOC_MAX_NBAS);
         return 3;
     }
+    // without Schwarz factors the kernels would screen nothing at all
+    if (pair_q == nullptr) return 3;
     double *dm_cond = noalloc_scratch();
     if (dm_cond == nullptr) return 1;
     // every entry of the nbas x nbas table is overwritten before it is read

@@ -26,6 +26,7 @@
 // same pair (a == b), and the 1/2 of a diagonal shell pair carried in e12.
 #pragma once
 #include <stdio.h>
+#include <atomic>
 #include "jk_device.cuh"
 
 namespace bqc {
@@ -33,6 +34,47 @@ namespace bqc {
 constexpr int TILE = 16;
 constexpr int SMALL_NF = 54;
 constexpr double TWO_PI_2P5 = 34.986836655249725693;  // 2 pi^(5/2)
+
+// 8-byte asynchronous global -> shared copies (cp.async, completed by the
+// issuing thread's wait): the density blocks a quartet digests are fetched
+// while its integrals are evaluated.
+__device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// The six density blocks one quartet (i j | k l) digests, in one private
+// shared-memory record per thread: D_kl (NFK x NFL), D_ij, D_ik, D_il, D_jk,
+// D_jl, row-major within each block, starting at the offsets below.
+template <int NFI, int NFJ, int NFK, int NFL>
+struct DmRecord {
+    static constexpr int KL = 0, IJ = KL + NFK * NFL, IK = IJ + NFI * NFJ, IL = IK + NFI * NFK,
+                         JK = IL + NFI * NFL, JL = JK + NFJ * NFK, SIZE = JL + NFJ * NFL;
+    // odd stride: the records of neighbouring lanes start in different banks
+    static constexpr int STRIDE = SIZE | 1;
+
+    template <int NR, int NC>
+    static __device__ __forceinline__ void copy_block(double *dst, const double *__restrict__ D,
+                                                      int nao, int r0, int c0) {
+#pragma unroll
+        for (int r = 0; r < NR; r++)
+#pragma unroll
+            for (int c = 0; c < NC; c++) cp_async8(dst + r * NC + c, D + (size_t)(r0 + r) * nao + c0 + c);
+    }
+    // issue the copies of the record of quartet (i0, j0, k0, l0) (first AOs)
+    static __device__ __forceinline__ void stage(double *rec, const double *__restrict__ D, int nao,
+                                                 int i0, int j0, int k0, int l0) {
+        copy_block<NFK, NFL>(rec + KL, D, nao, k0, l0);
+        copy_block<NFI, NFJ>(rec + IJ, D, nao, i0, j0);
+        copy_block<NFI, NFK>(rec + IK, D, nao, i0, k0);
+        copy_block<NFI, NFL>(rec + IL, D, nao, i0, l0);
+        copy_block<NFJ, NFK>(rec + JK, D, nao, j0, k0);
+        copy_block<NFJ, NFL>(rec + JL, D, nao, j0, l0);
+        cp_async_commit();
+    }
+};
 
 // ---------------------------------------------------------------------------
 // tile screening: returns false (uniformly) if the tile holds no quartet
@@ -287,6 +329,12 @@ jk_tile(JKArgs A, JKTask T) {
     }
     if (!__syncthreads_or(active)) return;
 
+    // the first density's blocks are copied while the integrals are evaluated
+    using R = DmRecord<NFI, NFJ, NFK, NFL>;
+    extern __shared__ double s_dm[];
+    double *rec = s_dm + threadIdx.x * R::STRIDE;
+    if (active && A.eri == nullptr) R::stage(rec, A.dm, A.nao, Q.i0, Q.j0, Q.k0, Q.l0);
+
     F acc[NF];
 #pragma unroll
     for (int n = 0; n < NF; n++) acc[n] = F(0);
@@ -365,8 +413,10 @@ jk_tile(JKArgs A, JKTask T) {
     const int i0t = __ldg(A.ao_loc + i_tile), k0t = __ldg(A.ao_loc + k_tile) + K0;
 #define ACC(fi, fj, fk, fl) ((double)acc[(((fi) * NFJ + (fj)) * NFK + (fk)) * NFL + (fl)])
     for (int id = 0; id < A.n_dm; id++) {
-        const double *__restrict__ D = A.dm + id * nn;
-        auto ld = [&](int r0, int c0) { return __ldg(D + (size_t)r0 * nao + c0); };
+        // density blocks of this quartet: staged for the first density at the
+        // start of the kernel, fetched here for the others
+        if (id > 0 && active) R::stage(rec, A.dm + id * nn, nao, Q.i0, Q.j0, Q.k0, Q.l0);
+        cp_async_wait_all();
         if (A.vj != nullptr) {
             double *VJ = A.vj + id * nn;
             double pij[NIJ];
@@ -375,7 +425,7 @@ jk_tile(JKArgs A, JKTask T) {
             if (active) {
 #pragma unroll
                 for (int kl = 0; kl < NKL; kl++) {
-                    const double d = ld(Q.k0 + kl / NFL, Q.l0 + kl % NFL);
+                    const double d = rec[R::KL + kl];
 #pragma unroll
                     for (int ij = 0; ij < NIJ; ij++) pij[ij] += (double)acc[ij * NKL + kl] * d;
                 }
@@ -394,7 +444,7 @@ jk_tile(JKArgs A, JKTask T) {
             if (active) {
 #pragma unroll
                 for (int ij = 0; ij < NIJ; ij++) {
-                    const double d = ld(Q.i0 + ij / NFJ, Q.j0 + ij % NFJ);
+                    const double d = rec[R::IJ + ij];
 #pragma unroll
                     for (int kl = 0; kl < NKL; kl++) pkl[kl] += (double)acc[ij * NKL + kl] * d;
                 }
@@ -419,7 +469,7 @@ jk_tile(JKArgs A, JKTask T) {
                 for (int fi = 0; fi < NFI; fi++)
 #pragma unroll
                     for (int fk = 0; fk < NFK; fk++) {
-                        const double d = ld(Q.i0 + fi, Q.k0 + fk);
+                        const double d = rec[R::IK + fi * NFK + fk];
 #pragma unroll
                         for (int fj = 0; fj < NFJ; fj++)
 #pragma unroll
@@ -439,7 +489,7 @@ jk_tile(JKArgs A, JKTask T) {
                     for (int fi = 0; fi < NFI; fi++)
 #pragma unroll
                         for (int fl = 0; fl < NFL; fl++) {
-                            const double d = ld(Q.i0 + fi, Q.l0 + fl);
+                            const double d = rec[R::IL + fi * NFL + fl];
 #pragma unroll
                             for (int fj = 0; fj < NFJ; fj++)
 #pragma unroll
@@ -470,7 +520,7 @@ jk_tile(JKArgs A, JKTask T) {
                     for (int fj = 0; fj < NFJ; fj++)
 #pragma unroll
                         for (int fk = 0; fk < NFK; fk++) {
-                            const double d = ld(Q.j0 + fj, Q.k0 + fk);
+                            const double d = rec[R::JK + fj * NFK + fk];
 #pragma unroll
                             for (int fi = 0; fi < NFI; fi++)
 #pragma unroll
@@ -501,7 +551,7 @@ jk_tile(JKArgs A, JKTask T) {
                     for (int fj = 0; fj < NFJ; fj++)
 #pragma unroll
                         for (int fl = 0; fl < NFL; fl++) {
-                            const double d = ld(Q.j0 + fj, Q.l0 + fl);
+                            const double d = rec[R::JL + fj * NFL + fl];
 #pragma unroll
                             for (int fi = 0; fi < NFI; fi++)
 #pragma unroll
@@ -590,7 +640,7 @@ __global__ void __launch_bounds__(GroupCfg<LI, LJ, LK, LL, NSPLIT>::NT,
 jk_group(JKArgs A, JKTask T) {
     using C = GroupCfg<LI, LJ, LK, LL, NSPLIT>;
     constexpr int NFI = C::NFI, NFJ = C::NFJ, NFK = C::NFK, NFL = C::NFL;
-    constexpr int NR = C::NR, TPQ = C::TPQ, NG = C::NG, GSZ = C::GSZ, CK = C::CK;
+    constexpr int NR = C::NR, TPQ = C::TPQ, NG = C::NG, CK = C::CK;
     extern __shared__ double smem[];
     __shared__ int s_list[TILE * TILE];
     __shared__ int s_count;
@@ -642,6 +692,23 @@ jk_group(JKArgs A, JKTask T) {
         F acc[C::NACC];
 #pragma unroll
         for (int n = 0; n < C::NACC; n++) acc[n] = F(0);
+        // The six density blocks of this quartet, lane-strided over the group
+        // into dbuf (which the 2D tables do not touch); the first density's
+        // copies run while the integrals are evaluated.
+        auto stage = [&](const double *__restrict__ D) {
+            for (int e = lane; e < C::DBUF; e += TPQ) {
+                int r0 = 0, c0 = 0, nc = 1, o = e;
+                if (o < C::NIJ) { r0 = Q.i0; c0 = Q.j0; nc = NFJ; }
+                else if ((o -= C::NIJ) < C::NKL) { r0 = Q.k0; c0 = Q.l0; nc = NFL; }
+                else if ((o -= C::NKL) < NFI * NFK) { r0 = Q.i0; c0 = Q.k0; nc = NFK; }
+                else if ((o -= NFI * NFK) < NFI * NFL) { r0 = Q.i0; c0 = Q.l0; nc = NFL; }
+                else if ((o -= NFI * NFL) < NFJ * NFK) { r0 = Q.j0; c0 = Q.k0; nc = NFK; }
+                else { o -= NFJ * NFK; r0 = Q.j0; c0 = Q.l0; nc = NFL; }
+                cp_async8(dbuf + e, D + (size_t)(r0 + o / nc) * A.nao + c0 + o % nc);
+            }
+            cp_async_commit();
+        };
+        if (active && A.eri == nullptr) stage(A.dm);
 
         for (int ip = 0; ip < T.nprim_a; ip++) {
             for (int kp = 0; kp < T.nprim_b; kp++) {
@@ -739,19 +806,8 @@ jk_group(JKArgs A, JKTask T) {
         const int nao = A.nao;
         const size_t nn = (size_t)nao * nao;
         for (int id = 0; id < A.n_dm; id++) {
-            const double *__restrict__ D = A.dm + id * nn;
-            if (active) {
-                for (int e = lane; e < C::DBUF; e += TPQ) {
-                    int r0 = 0, c0 = 0, nc = 1, o = e;
-                    if (o < C::NIJ) { r0 = Q.i0; c0 = Q.j0; nc = NFJ; }
-                    else if ((o -= C::NIJ) < C::NKL) { r0 = Q.k0; c0 = Q.l0; nc = NFL; }
-                    else if ((o -= C::NKL) < NFI * NFK) { r0 = Q.i0; c0 = Q.k0; nc = NFK; }
-                    else if ((o -= NFI * NFK) < NFI * NFL) { r0 = Q.i0; c0 = Q.l0; nc = NFL; }
-                    else if ((o -= NFI * NFL) < NFJ * NFK) { r0 = Q.j0; c0 = Q.k0; nc = NFK; }
-                    else { o -= NFJ * NFK; r0 = Q.j0; c0 = Q.l0; nc = NFL; }
-                    dbuf[e] = __ldg(D + (size_t)(r0 + o / nc) * nao + c0 + o % nc);
-                }
-            }
+            if (id > 0 && active) stage(A.dm + id * nn);
+            cp_async_wait_all();
             __syncthreads();
             if (A.vj != nullptr && active) {
                 double s = 0;
@@ -871,30 +927,56 @@ static inline int task_tiles(const JKTask &task) {
     return ((task.na + TILE - 1) / TILE) * ((task.nb + TILE - 1) / TILE);
 }
 
-template <int LI, int LJ, int LK, int LL, typename F>
-static void launch_tile_f(const JKArgs &args, const JKTask &task, int ntiles, cudaStream_t stream) {
-    jk_tile<LI, LJ, LK, LL, F><<<ntiles, 256, 0, stream>>>(args, task);
+// Raise the dynamic shared-memory limit of kernel K to `bytes`, once per
+// device: the attribute belongs to the (kernel, device) pair, so a process
+// that drives several GPUs sets it on each (flags per device, race-free).
+constexpr int MAX_DEVICES = 64;
+template <auto K>
+static int smem_attr(int bytes) {
+    static std::atomic<unsigned char> done[MAX_DEVICES];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return 1;
+    if (!done[dev].load(std::memory_order_acquire)) {
+        if (cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+            return 1;
+        done[dev].store(1, std::memory_order_release);
+    }
+    return 0;
+}
+
+// dynamic shared memory of a jk_tile launch: one density record per thread
+template <int LI, int LJ, int LK, int LL, int KN>
+constexpr int tile_smem() {
+    return 256 * DmRecord<ncart(LI), ncart(LJ), KN, ncart(LL)>::STRIDE * (int)sizeof(double);
+}
+
+template <int LI, int LJ, int LK, int LL, typename F, int K0, int KN>
+static int launch_tile_range(const JKArgs &args, const JKTask &task, int ntiles, cudaStream_t stream) {
+    constexpr int SMEM = tile_smem<LI, LJ, LK, LL, KN>();
+    static_assert(SMEM <= 200 * 1024, "density records per CTA");
+    if (smem_attr<jk_tile<LI, LJ, LK, LL, F, K0, KN>>(SMEM)) return 1;
+    jk_tile<LI, LJ, LK, LL, F, K0, KN><<<ntiles, 256, SMEM, stream>>>(args, task);
+    return 0;
 }
 
 template <int LI, int LJ, int LK, int LL>
 static int launch_small(const JKArgs &args, const JKTask &task, int fp32, cudaStream_t stream) {
     int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
     if (ntiles == 0) return 0;
-    if (fp32)
-        launch_tile_f<LI, LJ, LK, LL, float>(args, task, ntiles, stream);
-    else
-        launch_tile_f<LI, LJ, LK, LL, double>(args, task, ntiles, stream);
-    return 0;
+    constexpr int KN = ncart(LK);
+    if (fp32) return launch_tile_range<LI, LJ, LK, LL, float, 0, KN>(args, task, ntiles, stream);
+    return launch_tile_range<LI, LJ, LK, LL, double, 0, KN>(args, task, ntiles, stream);
 }
 
 // Ket-split tile launches: jk_tile over fk in [K0, K0 + CK), [K0 + CK, ...)
 // until shell k is covered (one launch each).
 template <int LI, int LJ, int LK, int LL, typename F, int K0, int CK>
-static void launch_split_f(const JKArgs &args, const JKTask &task, int ntiles, cudaStream_t stream) {
+static int launch_split_f(const JKArgs &args, const JKTask &task, int ntiles, cudaStream_t stream) {
     constexpr int KN = imin(CK, ncart(LK) - K0);
-    jk_tile<LI, LJ, LK, LL, F, K0, KN><<<ntiles, 256, 0, stream>>>(args, task);
+    if (launch_tile_range<LI, LJ, LK, LL, F, K0, KN>(args, task, ntiles, stream)) return 1;
     if constexpr (K0 + CK < ncart(LK))
-        launch_split_f<LI, LJ, LK, LL, F, K0 + CK, CK>(args, task, ntiles, stream);
+        return launch_split_f<LI, LJ, LK, LL, F, K0 + CK, CK>(args, task, ntiles, stream);
+    return 0;
 }
 
 template <int LI, int LJ, int LK, int LL, int CK>
@@ -902,11 +984,8 @@ static int launch_split(const JKArgs &args, const JKTask &task, int fp32, cudaSt
     int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
     if (ntiles == 0) return 0;
     bqc_count_launch(cdiv(ncart(LK), CK) - 1);   // the dispatcher counted one
-    if (fp32)
-        launch_split_f<LI, LJ, LK, LL, float, 0, CK>(args, task, ntiles, stream);
-    else
-        launch_split_f<LI, LJ, LK, LL, double, 0, CK>(args, task, ntiles, stream);
-    return 0;
+    if (fp32) return launch_split_f<LI, LJ, LK, LL, float, 0, CK>(args, task, ntiles, stream);
+    return launch_split_f<LI, LJ, LK, LL, double, 0, CK>(args, task, ntiles, stream);
 }
 
 template <int LI, int LJ, int LK, int LL, int NSPLIT, typename F>
@@ -916,12 +995,7 @@ static int launch_group_f(const JKArgs &args, const JKTask &task, cudaStream_t s
     static_assert(C::NT <= 1024, "threads per CTA");
     int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
     if (ntiles == 0) return 0;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(jk_group<LI, LJ, LK, LL, NSPLIT, F>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-        configured = true;
-    }
+    if (smem_attr<jk_group<LI, LJ, LK, LL, NSPLIT, F>>((int)C::SMEM)) return 1;
     jk_group<LI, LJ, LK, LL, NSPLIT, F><<<ntiles, C::NT, C::SMEM, stream>>>(args, task);
     return 0;
 }

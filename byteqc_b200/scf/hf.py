@@ -266,10 +266,20 @@ class _VHFOpt:
         return bp_cpu, bp_gpu, mem, keep
 
     def _free_cache(self, bp_cpu, bp_gpu):
+        """Release both structs.  The device copy shares the host blocks of
+        the cpu cache, so deleting it frees them (cuobc/scf/hf.py:439-442
+        deletes only that copy); the cpu struct is then released with its
+        shared pointers cleared."""
         lib = _libmod.load_library()
-        if bp_gpu:
+        shared = bool(bp_gpu)
+        if shared:
             lib.GINTdel_basis_prod(ctypes.byref(bp_gpu))
         if bp_cpu:
+            if shared:
+                c = bp_cpu.contents
+                c.cptype = None
+                c.primitive_pairs_locs = None
+                c.aexyz = None
             lib.GINTdel_basis_prod(ctypes.byref(bp_cpu))
 
     # -- build -----------------------------------------------------------------
@@ -611,6 +621,17 @@ class RHF(_SCFBase):
         from .guess import init_guess
         return init_guess(self, self.init_guess)
 
+    def get_veff(self, mol=None, dm=None, dm_last=0, vhf_last=0, hermi=1):
+        """Hartree-Fock potential J - K/2 (host arrays), pyscf's RHF.get_veff,
+        which the reference's RHF inherits (cuobc/scf/hf.py:272-274): with a
+        previous density and potential only the difference density goes
+        through get_jk (direct SCF) and the result is added to vhf_last."""
+        if dm is None:
+            raise ValueError('get_veff needs a density')
+        ddm = np.asarray(dm) - np.asarray(dm_last)
+        vj, vk = self.get_jk(mol, ddm, hermi)
+        return np.asarray(vhf_last) + vj - .5 * vk
+
     def make_rdm1(self, mo_coeff, mo_occ):
         c = mo_coeff[:, mo_occ > 0]
         return (c * mo_occ[mo_occ > 0]) @ c.T
@@ -789,6 +810,20 @@ class UHF(_SCFBase):
     through the n_dm batch dimension (no reference counterpart)."""
 
     rebuild_cycle = 8
+
+    def get_veff(self, mol=None, dm=None, dm_last=0, vhf_last=0, hermi=1):
+        """Alpha and beta potentials J(total) - K(spin) (host arrays, shape
+        (2, nao, nao)), pyscf's UHF.get_veff: the difference of the spin
+        densities against dm_last goes through one get_jk call (n_dm = 2)
+        and is added to vhf_last."""
+        if dm is None:
+            raise ValueError('get_veff needs a density')
+        dm = np.asarray(dm)
+        if dm.ndim != 3 or dm.shape[0] != 2:
+            raise ValueError('UHF.get_veff needs alpha and beta densities (2, nao, nao)')
+        ddm = dm - np.asarray(dm_last)
+        vj, vk = self.get_jk(mol, ddm, hermi)
+        return np.asarray(vhf_last) + (vj[0] + vj[1])[None] - vk
 
     def kernel(self, dm0=None):
         t0 = time.perf_counter()

@@ -170,7 +170,8 @@ int BQCint1e(const int *atm, int natm, const int *bas, int nbas, const double *e
  * scratch is a fixed array inside the library (2 MiB per GPU, held until the
  * process exits), so it accepts at most 512 shells of the sorted, decontracted
  * basis and returns 3 beyond that; it screens on the device against
- * q_ij q_kl max|D| >= tol and launches every quartet tile.  The first call on
+ * q_ij q_kl max|D| >= tol (pair_q is required: NULL returns 3) and launches
+ * every quartet tile.  The first call on
  * a device looks up the array's device address; make that first call before
  * any stream capture.  All calls share the array: calls that overlap on the
  * GPU (different streams, or concurrent host threads) race on it. */

@@ -4,9 +4,10 @@
 # the read-only reference tree, into oracle/_ref/ (git-ignored).  They serve
 # as a second checker: a GPU test drives the reference's GINTbuild_jk through
 # the same C ABI as this package's and compares J/K.  Test infrastructure
-# only.  Usage: bash oracle/build_ref.sh [reference root]
+# only.  Usage: bash oracle/build_ref.sh [reference root]; the root defaults
+# to $BYTEQC_REFERENCE_ROOT, else to where this build image mounts it.
 set -e
-REF=${1:-/root/reference}
+REF=${1:-${BYTEQC_REFERENCE_ROOT:-/root/reference}}
 SRC=$REF/cuobc/lib
 OUT=$(cd "$(dirname "$0")" && pwd)/_ref
 [ -d "$SRC/gint" ] || { echo "reference sources not found under $SRC"; exit 0; }

@@ -184,3 +184,53 @@ def rhf(mol, conv_tol=1e-10, max_cycle=100, dm0=None, nthreads=0):
         Fd = sum(ci * fi for ci, fi in zip(c, focks))
         dm = new_dm(Fd)
     raise RuntimeError('oracle RHF did not converge')
+
+
+def uhf(mol, conv_tol=1e-10, max_cycle=200, dm0=None, nthreads=0):
+    """Unrestricted HF with DIIS on the stacked alpha/beta commutators.
+    Returns (energy, (dm_alpha, dm_beta), n_iterations).  dm0: initial
+    (2, nao, nao) densities (default: core-Hamiltonian orbitals filled with
+    nalpha / nbeta electrons).  The potentials follow pyscf's UHF:
+    F_s = h + J(dm_a + dm_b) - K(dm_s)."""
+    S, T, V = int1e(mol)
+    h = T + V
+    e_nuc = mol.energy_nuc()
+    seig, U = np.linalg.eigh(S)
+    keep = seig > 1e-15
+    X = U[:, keep] / np.sqrt(seig[keep])
+    na, nb = mol.nelec
+
+    def new_dm(F, n):
+        e, c = np.linalg.eigh(X.T @ F @ X)
+        c = X @ c
+        return c[:, :n] @ c[:, :n].T
+
+    if dm0 is None:
+        dm = np.stack([new_dm(h, na), new_dm(h, nb)])
+    else:
+        dm = np.asarray(dm0, dtype=np.float64)
+    e_last = 0.
+    focks, errs = [], []
+    for it in range(max_cycle):
+        vj, vk = get_jk(mol, dm, nthreads)
+        F = np.stack([h + vj[0] + vj[1] - vk[s] for s in range(2)])
+        e = .5 * sum(np.sum(dm[s] * (h + F[s])) for s in range(2)) + e_nuc
+        if abs(e - e_last) < conv_tol and it > 0:
+            return e, dm, it + 1
+        e_last = e
+        err = np.concatenate([(X.T @ (F[s] @ dm[s] @ S - S @ dm[s] @ F[s]) @ X).ravel()
+                              for s in range(2)])
+        focks.append(F)
+        errs.append(err)
+        focks, errs = focks[-8:], errs[-8:]
+        nd = len(focks)
+        B = -np.ones((nd + 1, nd + 1))
+        B[nd, nd] = 0
+        E = np.array(errs)
+        B[:nd, :nd] = E @ E.T
+        rhs = np.zeros(nd + 1)
+        rhs[nd] = -1
+        c = np.linalg.solve(B, rhs)[:nd]
+        Fd = sum(ci * fi for ci, fi in zip(c, focks))
+        dm = np.stack([new_dm(Fd[0], na), new_dm(Fd[1], nb)])
+    raise RuntimeError('oracle UHF did not converge')

@@ -1,7 +1,10 @@
 """Parity of the device J/K engine with the CPU oracle (needs a B200).
 
 Tolerances: J and K max-abs error <= 1e-10 in plain FP64 (the bar of the
-drop-in), SCF total energy within 1e-9 Eh.
+drop-in), SCF total energy within 1e-9 Eh.  Where a test's density makes |J|
+reach several hundred, the 1e-10 bar applies to J/max(1, |J|max/100): both
+sides sum O(10^5) FP64 terms per element, whose rounding alone reaches a few
+1e-15 relative; every such case states it.
 """
 import numpy as np
 import pytest
@@ -35,8 +38,11 @@ def test_jk_water(cuda, kind):
     dm = _rand_dm(mol.nao)
     vj, vk = hf.get_jk(mol, dm)
     rj, rk = oracle.get_jk(mol, dm)
-    assert abs(vj - rj).max() < TOL_JK * max(1, abs(rj).max() / 100)
-    assert abs(vk - rk).max() < TOL_JK * max(1, abs(rk).max() / 100)
+    ej, ek = abs(vj - rj).max(), abs(vk - rk).max()
+    print('water %s: max|J| %.3g max|dJ| %.3e max|dK| %.3e' % (kind, abs(rj).max(), ej, ek))
+    # |J| reaches ~400 with this density: relative bar (module doc)
+    assert ej < TOL_JK * max(1, abs(rj).max() / 100)
+    assert ek < TOL_JK * max(1, abs(rk).max() / 100)
 
 
 @pytest.mark.parametrize('variant', [1, 2])
@@ -58,8 +64,9 @@ def test_jk_class_variants(cuda, variant):
         for sh in shapes:
             lib.BQCset_class_variant(*sh, 0)
     rj, rk = oracle.get_jk(mol, dm)
-    assert abs(vj - rj).max() < 1e-9
-    assert abs(vk - rk).max() < 1e-9
+    print('variant %d: max|dJ| %.3e max|dK| %.3e' % (variant, abs(vj - rj).max(), abs(vk - rk).max()))
+    assert abs(vj - rj).max() < TOL_JK
+    assert abs(vk - rk).max() < TOL_JK
     assert lib.BQCset_class_variant(0, 0, 0, 0, 7) == 3
     assert lib.BQCset_class_variant(4, 0, 0, 0, 1) == 2
 
@@ -92,8 +99,11 @@ def test_jk_two_waters_tz(cuda):
     dm = _rand_dm(mol.nao, 7)
     vj, vk = hf.get_jk(mol, dm)
     rj, rk = oracle.get_jk(mol, dm)
-    assert abs(vj - rj).max() < 1e-9
-    assert abs(vk - rk).max() < 1e-9
+    ej, ek = abs(vj - rj).max(), abs(vk - rk).max()
+    print('TZ dimer: max|J| %.3g max|dJ| %.3e max|dK| %.3e' % (abs(rj).max(), ej, ek))
+    # |J| reaches ~1e3 with this density: relative bar (module doc)
+    assert ej < TOL_JK * max(1, abs(rj).max() / 100)
+    assert ek < TOL_JK * max(1, abs(rk).max() / 100)
 
 
 def test_schwarz_and_int1e(cuda):
@@ -154,8 +164,11 @@ def test_gint_abi_matches_native(cuda):
     J = (C.T @ J[0] @ C).cpu().numpy()
     K = (C.T @ K[0] @ C).cpu().numpy()
     rj, rk = oracle.get_jk(mol, dm)
-    assert abs(J - rj).max() < 1e-9
-    assert abs(K - rk).max() < 1e-9
+    print('GINT ABI: max|J| %.3g max|dJ| %.3e max|dK| %.3e' % (abs(rj).max(), abs(J - rj).max(),
+                                                             abs(K - rk).max()))
+    # |J| reaches ~500 with this density: relative bar (module doc)
+    assert abs(J - rj).max() < TOL_JK * max(1, abs(rj).max() / 100)
+    assert abs(K - rk).max() < TOL_JK * max(1, abs(rk).max() / 100)
 
 
 def test_rhf_energy(cuda):
@@ -184,8 +197,10 @@ def test_alkane_631gss(cuda):
     dm = _rand_dm(mol.nao, 5) * 0.1
     vj, vk = hf.get_jk(mol, dm)
     rj, rk = oracle.get_jk(mol, dm)
-    assert abs(vj - rj).max() < TOL_JK * 10
-    assert abs(vk - rk).max() < TOL_JK * 10
+    print('ethane: max|J| %.3g max|dJ| %.3e max|dK| %.3e' % (abs(rj).max(), abs(vj - rj).max(),
+                                                           abs(vk - rk).max()))
+    assert abs(vj - rj).max() < TOL_JK
+    assert abs(vk - rk).max() < TOL_JK
 
 
 def test_mixed_precision_jk_error(cuda):

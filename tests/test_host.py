@@ -167,3 +167,113 @@ def test_autotune_variant_rule():
     assert both == [(1, 1, 1, 1), (2, 1, 1, 1), (2, 1, 2, 0), (2, 2, 1, 0),
                     (3, 0, 1, 1), (3, 0, 2, 0), (3, 0, 3, 0), (3, 1, 1, 0)]
     assert autotune.canonical(0, 1, 2, 2) == (2, 2, 1, 0)
+
+
+def test_basis_prod_ownership_reference_sequence():
+    """The reference's call sequence (cuobc/scf/hf.py:410-442): init_cpu,
+    init_gpu on device copies, then GINTdel_basis_prod on the device copy
+    only.  The device copy shares and frees the host blocks of the cpu
+    cache, so repeating the sequence does not grow the heap (the few bytes
+    of the cpu struct itself are left, as in the reference)."""
+    from byteqc_b200 import lib as L
+    from byteqc_b200.scf.hf import basis_seg_contraction
+    lib = L.load_library()
+    libc = ctypes.CDLL('libc.so.6')
+
+    class MallInfo2(ctypes.Structure):
+        _fields_ = [(n, ctypes.c_size_t) for n in
+                    ('arena', 'ordblks', 'smblks', 'hblks', 'hblkhd', 'usmblks', 'fsmblks',
+                     'uordblks', 'fordblks', 'keepcost')]
+    libc.mallinfo2.restype = MallInfo2
+    mol = Mole(water_cluster(4, seed=1), synthetic_basis('cc-pvtz', ['O', 'H']))
+    pmol, _ = basis_seg_contraction(mol)
+    n = pmol.nbas
+    # one class: all pairs of the shells of one (l, nprim) kind (the class
+    # table takes l and nprim from its first pair)
+    kind = pmol._bas[:, 1] * 100 + pmol._bas[:, 2]
+    sel = np.flatnonzero(kind == np.bincount(kind).argmax())
+    ii, jj = np.tril_indices(len(sel))
+    i, j = sel[ii], sel[jj]
+    p2s = np.ascontiguousarray(np.vstack([i, j]), dtype=np.int32)
+    locs = np.array([0, len(i)], dtype=np.int32)
+    atm = np.ascontiguousarray(pmol._atm, dtype=np.int32)
+    bas = np.ascontiguousarray(pmol._bas, dtype=np.int32)
+    env = np.ascontiguousarray(pmol._env)
+    coords = np.empty(3 * n)
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+
+    def sequence():
+        bp = ctypes.POINTER(L.BasisProdCache)()
+        lib.GINTinit_basis_prod_cpu(ctypes.byref(bp), ctypes.c_double(.5), vp(coords), vp(p2s),
+                                    vp(locs), ctypes.c_int(1), vp(atm), ctypes.c_int(pmol.natm),
+                                    vp(bas), ctypes.c_int(n), vp(env))
+        assert bp.contents.aexyz    # the host block the cpu cache fills
+        bpg = ctypes.POINTER(L.BasisProdCache)()
+        # device pointers are only stored, never dereferenced on the host
+        lib.GINTinit_basis_prod_gpu(ctypes.byref(bp), ctypes.byref(bpg), None, None, None, None)
+        assert ctypes.cast(bpg.contents.aexyz, ctypes.c_void_p).value == \
+            ctypes.cast(bp.contents.aexyz, ctypes.c_void_p).value
+        lib.GINTdel_basis_prod(ctypes.byref(bpg))
+        assert not bpg
+
+    for _ in range(5):
+        sequence()
+    used0 = libc.mallinfo2().uordblks + libc.mallinfo2().hblkhd
+    for _ in range(50):
+        sequence()
+    used1 = libc.mallinfo2().uordblks + libc.mallinfo2().hblkhd
+    block = 5 * 8 * len(i)       # the aexyz block of one cache
+    assert used1 - used0 < block, (used1 - used0, block)
+
+
+def test_reference_decontraction_matches_engine():
+    """The reference-side restatement (oracle/ref_gpu.py seg_contraction of
+    cuobc/scf/hf.py:481-564) and the engine's basis_seg_contraction give the
+    same primitive basis and contraction matrix."""
+    from byteqc_b200.scf.hf import basis_seg_contraction
+    from oracle.ref_gpu import seg_contraction
+    for kind in ('cc-pvdz', 'cc-pvtz'):
+        mol = Mole(water_cluster(2, seed=4), synthetic_basis(kind, ['O', 'H']))
+        p1, c1 = basis_seg_contraction(mol)
+        p2, c2 = seg_contraction(mol)
+        assert (p1._bas == p2._bas).all()
+        assert np.allclose(p1._env, p2._env, rtol=1e-15, atol=0)
+        assert np.allclose(c1, c2, rtol=1e-14, atol=1e-15)
+
+
+def test_reference_pair_lists():
+    """RefVHFOpt (cuobc/scf/hf.py:288-397 restated): per class the pairs
+    above the cutoff in descending q, ish >= jsh on diagonal blocks, every
+    pair listed exactly once, log q clipped at 0."""
+    from oracle.ref_gpu import RefVHFOpt
+    mol = Mole(water_cluster(3, seed=6), synthetic_basis('cc-pvdz', ['O', 'H']))
+    opt = RefVHFOpt(mol).build(1e-13)
+    q = oracle.q_cond(opt.mol)
+    offs = opt.l_ctr_offsets
+    seen = set()
+    c = 0
+    for p in range(len(opt.uniq_l_ctr)):
+        for r in range(p + 1):
+            sl = slice(opt.bas_pairs_locs[c], opt.bas_pairs_locs[c + 1])
+            bra, ket = opt.bas_pair2shls[0, sl], opt.bas_pair2shls[1, sl]
+            assert ((bra >= offs[p]) & (bra < offs[p + 1])).all()
+            assert ((ket >= offs[r]) & (ket < offs[r + 1])).all()
+            qs = q[bra, ket]
+            assert (np.diff(qs) <= 0).all() and (qs > 1e-13).all()
+            if p == r:
+                assert (bra >= ket).all()
+            assert np.allclose(opt.log_qs[c], np.minimum(np.log(qs), 0))
+            seen.update(zip(bra.tolist(), ket.tolist()))
+            c += 1
+    n = opt.mol.nbas
+    expect = {(i, j) if opt_i_ge(i, j, offs) else (j, i) for i in range(n) for j in range(n)
+              if q[i, j] > 1e-13}
+    assert seen == expect
+
+
+def opt_i_ge(i, j, offs):
+    """Orientation of a pair in the reference lists: the bra shell comes from
+    the later (l, nprim) group, or is the larger index within one group."""
+    gi = np.searchsorted(offs, i, side='right')
+    gj = np.searchsorted(offs, j, side='right')
+    return gi > gj or (gi == gj and i >= j)

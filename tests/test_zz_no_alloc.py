@@ -87,3 +87,73 @@ def test_noalloc_rejects_basis_beyond_limit():
     err, vj, vk = _build(lib, opt, dmc, noalloc=True)
     assert err == 3
     assert float(vj.abs().max()) == 0.0
+
+
+def _driver_pool_high(dev=0):
+    """Used-memory high watermark of the device's default stream-ordered
+    memory pool (driver API), which cudaMallocAsync draws from."""
+    import ctypes
+    cu = ctypes.CDLL('libcuda.so.1')
+    pool = ctypes.c_void_p()
+    assert cu.cuDeviceGetDefaultMemPool(ctypes.byref(pool), ctypes.c_int(dev)) == 0
+    val = ctypes.c_uint64(0)
+    CU_MEMPOOL_ATTR_USED_MEM_HIGH = 8
+    assert cu.cuMemPoolGetAttribute(pool, ctypes.c_int(CU_MEMPOOL_ATTR_USED_MEM_HIGH),
+                                    ctypes.byref(val)) == 0
+    return cu, pool, val.value
+
+
+def _reset_pool_high(cu, pool):
+    import ctypes
+    zero = ctypes.c_uint64(0)
+    assert cu.cuMemPoolSetAttribute(pool, ctypes.c_int(8), ctypes.byref(zero)) == 0
+
+
+def test_noalloc_allocates_nothing():
+    """After a warm-up call, two more calls leave the device's free memory
+    and the default memory pool's high watermark unchanged, while the
+    allocating entry point does raise that watermark (so the probe sees
+    stream-ordered allocations); a NULL pair_q is refused."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip('no CUDA device')
+    from byteqc_b200 import lib as L
+    from byteqc_b200.scf import hf
+    lib = L.load_library()
+    mol = Mole(water_cluster(2, seed=9), synthetic_basis('cc-pvdz', ['O', 'H']))
+    opt = hf._VHFOpt(mol).build()
+    rng = np.random.default_rng(6)
+    dm = rng.random((mol.nao, mol.nao))
+    C = opt.coeff_dev
+    dmc = (C @ torch.as_tensor(dm + dm.T, device='cuda') @ C.T)[None].contiguous()
+    vj = torch.zeros_like(dmc)
+    vk = torch.zeros_like(dmc)
+    bp = ctypes.cast(opt.bpcache, ctypes.c_void_p)
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+    def call():
+        vj.zero_()
+        vk.zero_()
+        err = lib.BQCbuild_jk_noalloc(bp, _vp(opt.pair_q), _vp(vj), _vp(vk), _vp(dmc),
+                                      ctypes.c_int(dmc.shape[-1]), ctypes.c_int(1),
+                                      ctypes.c_double(opt.direct_scf_tol), stream)
+        torch.cuda.synchronize()
+        return err
+
+    assert call() == 0   # warm-up: the device address look-up
+    cu, pool, _ = _driver_pool_high()
+    _reset_pool_high(cu, pool)
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(2):
+        assert call() == 0
+    free1 = torch.cuda.mem_get_info()[0]
+    _, _, high = _driver_pool_high()
+    assert high == 0, high
+    assert free1 == free0
+    err, _, _ = _build(lib, opt, dmc, noalloc=False)      # positive control
+    assert err == 0
+    _, _, high = _driver_pool_high()
+    assert high > 0
+    # no Schwarz factors: refused
+    assert lib.BQCbuild_jk_noalloc(bp, None, _vp(vj), _vp(vk), _vp(dmc), ctypes.c_int(dmc.shape[-1]),
+                                   ctypes.c_int(1), ctypes.c_double(1e-13), stream) == 3
