@@ -385,6 +385,9 @@ def extras(args, mol, mf, e, t_step, line, lib):
     line['jk_build'] = {'s': round(time_build(lambda: opt.jk_cart(dmc)), 3),
                         'density': JKPY_DENSITY, 'tol': opt.direct_scf_tol}
     line['jk_build']['reference_check'] = reference_check(args, opt, dmc, e_p)
+    # the batched form on its own configuration: 256 seeded (H2O)_k, k in
+    # [1, 12], cc-pVDZ shape, in one batched solve, against one-by-one solves
+    line['batched'] = batched_leg()
     # CPU baseline: the oracle on a bounded sample, host cores
     threads = os.cpu_count() or 1
     t_cpu, e_cpu, cyc, desc = cpu_oracle_scf(threads)
@@ -408,6 +411,38 @@ def extras(args, mol, mf, e, t_step, line, lib):
     torch.cuda.synchronize()
     line['cpu_baseline']['same_sample_on_gpu_s'] = round(ev0.elapsed_time(ev1) / 1e3, 3)
     line['cpu_baseline']['energy_diff_gpu_vs_oracle'] = abs(e_s - e_cpu)
+
+
+def batched_leg(nmol=256, nseq=64, conv=1e-8):
+    """Molecules/s of one batched solve of nmol seeded (H2O)_k (k uniform in
+    [1, 12], cc-pVDZ shape) against one-by-one plain solves of the first nseq
+    of them, and the largest energy difference between the two."""
+    import torch
+    from byteqc_b200.scf import batched, hf, guess
+    mols = batched.batch_systems(nmol)
+    batched.BatchedRHF(mols[:2]).kernel()     # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    mf = batched.BatchedRHF(mols)
+    mf.conv_tol = conv
+    e = mf.kernel()
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    es = []
+    t0 = time.perf_counter()
+    for m in mols[:nseq]:
+        one = hf.RHF(m)
+        one.conv_tol = conv
+        es.append(one.kernel())
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    return {'config': '%d x (H2O)_k, k uniform in [1, 12], cc-pvdz-shaped (%d AO in total)' % (
+                nmol, sum(m.nao for m in mols)),
+            'batched_s': round(t_batch, 3), 'molecules_per_s': round(nmol / t_batch, 2),
+            'cycles': mf.cycles, 'converged': bool(mf.converged),
+            'sequential_molecules_per_s': round(nseq / t_seq, 2), 'sequential_timed': nseq,
+            'speedup': round((nmol / t_batch) / (nseq / t_seq), 3),
+            'max_energy_diff': float(np.max(np.abs(np.asarray(es) - np.asarray(e)[:nseq])))}
 
 
 REF_OUT = os.path.join(os.environ.get('TMPDIR', '/tmp'), 'byteqc_b200_reference_%s.npz')

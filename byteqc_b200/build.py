@@ -24,7 +24,7 @@ FLAGS = ['-O3', '-std=c++17', '-lineinfo', '-Xcompiler', '-fPIC', '-I', CSRC, '-
          '-ccbin', 'g++']
 
 PAIRS = [(0, 0), (1, 0), (1, 1), (2, 0), (2, 1), (2, 2), (3, 0), (3, 1), (3, 2), (3, 3)]
-SOURCES = ['jk_dispatch.cu', 'schwarz.cu', 'capi.cu', 'int1e.cu', 'rys_table.cu', 'peak.cu', 'mlp.cu']
+SOURCES = ['jk_dispatch.cu', 'schwarz.cu', 'capi.cu', 'int1e.cu', 'rys_table.cu', 'peak.cu', 'mlp.cu', 'plan.cu']
 
 
 def classes():

@@ -66,7 +66,22 @@ struct JKTask {
     int nrows;
     int ntiles;        // number of tiles (blocks) when tile_prefix is set
     int rows_are_b;
+    // Persistent launch: when set, the tile count lives on the device (a
+    // schedule computed there) and a fixed grid of CTAs strides over the
+    // tiles [0, *ntiles_dev); ntiles is then only an upper bound, and the
+    // grid holds at most a few CTAs per SM of the nsm SMs.
+    const int *ntiles_dev;
+    int nsm;
 };
+
+// grid of a launch over ntiles tiles of per_tile CTAs each; persistent
+// launches cap it at ctas_per_sm CTAs on each SM
+static inline int bqc_grid(const JKTask &t, int ntiles, int per_tile, int ctas_per_sm) {
+    const long long n = (long long)ntiles * per_tile;
+    if (t.ntiles_dev == nullptr) return (int)n;
+    const long long cap = (long long)t.nsm * ctas_per_sm;
+    return (int)(n < cap ? n : cap);
+}
 
 // number of kernel launches issued by the library so far (all threads)
 unsigned long long bqc_count_launch(int n);

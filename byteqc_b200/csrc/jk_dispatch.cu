@@ -115,9 +115,13 @@ int bqc_launch_dm_cond(const double *dm, int n_dm, int nao, const int *ao_loc, i
 __global__ void count_kernel(JKArgs A, JKTask T, unsigned long long *count) {
     __shared__ int s_list[bqc::TILE * bqc::TILE];
     __shared__ int s_count;
-    int a_begin, b_begin, n;
-    if (!bqc::tile_screen(A, T, s_list, &s_count, a_begin, b_begin, n)) return;
-    if (threadIdx.x == 0) atomicAdd(count, (unsigned long long)n);
+    const int ntiles = T.ntiles_dev != nullptr ? __ldg(T.ntiles_dev) : (int)gridDim.x;
+    for (int x = blockIdx.x; x < ntiles; x += gridDim.x) {
+        int a_begin, b_begin, n;
+        if (bqc::tile_screen(A, T, x, s_list, &s_count, a_begin, b_begin, n) && threadIdx.x == 0)
+            atomicAdd(count, (unsigned long long)n);
+        __syncthreads();
+    }
 }
 
 int bqc_launch_count(const JKArgs &args, const JKTask &task, unsigned long long *count,
@@ -125,6 +129,6 @@ int bqc_launch_count(const JKArgs &args, const JKTask &task, unsigned long long 
     int ntiles = task.tile_prefix ? task.ntiles : bqc::task_tiles(task);
     if (ntiles == 0) return 0;
     bqc_count_launch(1);
-    count_kernel<<<ntiles, 256, 0, stream>>>(args, task, count);
+    count_kernel<<<bqc_grid(task, ntiles, 1, 8), 256, 0, stream>>>(args, task, count);
     return cudaGetLastError() == cudaSuccess ? 0 : 1;
 }

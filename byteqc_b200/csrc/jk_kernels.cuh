@@ -7,11 +7,11 @@
 // q_ij q_kl max|D| >= tol (the six density blocks a quartet touches) and
 // evaluates the survivors:
 //
-// * jk_tile: one thread per quartet (16 x 16 threads per tile) for classes
-//   with at most SMALL_NF Cartesian components; the 2D integrals and the
-//   contracted quartet block live in registers, the six J/K targets are
-//   digested from registers with row / column / tile reductions where the
-//   tile's pairs share a target.
+// * jk_tile: one thread per quartet for classes with at most SMALL_NF
+//   Cartesian components, a tile run as two CTAs of 8 x 16 quartets; the 2D
+//   integrals and the contracted quartet block live in registers, the six J/K
+//   targets are digested from registers with row / column / CTA reductions
+//   where the CTA's pairs share a target.
 // * jk_group: the survivors are packed into a shared-memory list and each
 //   takes TPQ = nfi * nfj * NSPLIT threads; thread
 //   (fi, fj, chunk) owns the ket components (fk in its chunk, all fl) of bra
@@ -32,6 +32,13 @@
 namespace bqc {
 
 constexpr int TILE = 16;
+// jk_tile runs a 16 x 16 tile as two CTAs of 8 bra pairs x 16 ket pairs
+// (128 threads): two CTAs of the same size share an SM where one 256-thread
+// CTA fills the register file, so one CTA's reductions and barriers overlap
+// the other's integrals
+constexpr int TILE_ROWS = 8;
+constexpr int TILE_THREADS = TILE_ROWS * TILE;
+constexpr int TILE_WARPS = TILE_THREADS / 32;
 constexpr int SMALL_NF = 54;
 constexpr double TWO_PI_2P5 = 34.986836655249725693;  // 2 pi^(5/2)
 
@@ -44,37 +51,6 @@ __device__ __forceinline__ void cp_async8(double *smem, const double *gmem) {
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
-
-// The six density blocks one quartet (i j | k l) digests, in one private
-// shared-memory record per thread: D_kl (NFK x NFL), D_ij, D_ik, D_il, D_jk,
-// D_jl, row-major within each block, starting at the offsets below.
-template <int NFI, int NFJ, int NFK, int NFL>
-struct DmRecord {
-    static constexpr int KL = 0, IJ = KL + NFK * NFL, IK = IJ + NFI * NFJ, IL = IK + NFI * NFK,
-                         JK = IL + NFI * NFL, JL = JK + NFJ * NFK, SIZE = JL + NFJ * NFL;
-    // odd stride: the records of neighbouring lanes start in different banks
-    static constexpr int STRIDE = SIZE | 1;
-
-    template <int NR, int NC>
-    static __device__ __forceinline__ void copy_block(double *dst, const double *__restrict__ D,
-                                                      int nao, int r0, int c0) {
-#pragma unroll
-        for (int r = 0; r < NR; r++)
-#pragma unroll
-            for (int c = 0; c < NC; c++) cp_async8(dst + r * NC + c, D + (size_t)(r0 + r) * nao + c0 + c);
-    }
-    // issue the copies of the record of quartet (i0, j0, k0, l0) (first AOs)
-    static __device__ __forceinline__ void stage(double *rec, const double *__restrict__ D, int nao,
-                                                 int i0, int j0, int k0, int l0) {
-        copy_block<NFK, NFL>(rec + KL, D, nao, k0, l0);
-        copy_block<NFI, NFJ>(rec + IJ, D, nao, i0, j0);
-        copy_block<NFI, NFK>(rec + IK, D, nao, i0, k0);
-        copy_block<NFI, NFL>(rec + IL, D, nao, i0, l0);
-        copy_block<NFJ, NFK>(rec + JK, D, nao, j0, k0);
-        copy_block<NFJ, NFL>(rec + JL, D, nao, j0, l0);
-        cp_async_commit();
-    }
-};
 
 // ---------------------------------------------------------------------------
 // tile screening: returns false (uniformly) if the tile holds no quartet
@@ -94,9 +70,9 @@ __device__ __forceinline__ double dmax6(const double *__restrict__ dmc, int nbas
 // keeps the last one that qualifies, so a row index of up to 2^20 takes four
 // rounds of loads instead of twenty dependent ones.  All 32 lanes of every
 // warp must call it.
-__device__ __forceinline__ void tile_of_block(const JKTask &T, int &r, int &c) {
+__device__ __forceinline__ void tile_of_block(const JKTask &T, int x, int &r, int &c) {
     if (T.tile_prefix != nullptr) {
-        const int x = blockIdx.x, lane = threadIdx.x & 31;
+        const int lane = threadIdx.x & 31;
         int lo = 0, hi = T.nrows;   // tile_prefix[lo] <= x; answer in [lo, hi)
         while (hi - lo > 1) {
             const int step = (hi - lo + 31) >> 5;
@@ -111,16 +87,16 @@ __device__ __forceinline__ void tile_of_block(const JKTask &T, int &r, int &c) {
         if (T.tile_col0 != nullptr) c += __ldg(T.tile_col0 + r);
     } else {
         int ncols = ((T.rows_are_b ? T.na : T.nb) + TILE - 1) / TILE;
-        r = blockIdx.x / ncols;
-        c = blockIdx.x % ncols;
+        r = x / ncols;
+        c = x % ncols;
     }
 }
 
-__device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, int *s_list,
+__device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, int x, int *s_list,
                                             int *s_count, int &a_begin, int &b_begin,
                                             int &count) {
     int r, c;
-    tile_of_block(T, r, c);
+    tile_of_block(T, x, r, c);
     int ta = T.rows_are_b ? c : r, tb = T.rows_are_b ? r : c;
     a_begin = T.a0 + ta * TILE;
     b_begin = T.b0 + tb * TILE;
@@ -245,7 +221,7 @@ __device__ __forceinline__ void row_reduce(double (&v)[NV]) {
     }
 }
 
-// Sum v over the 16 rows of the tile for each column; afterwards threads
+// Sum v over the rows of the CTA for each column; afterwards threads
 // call emit(col, n, sum) for the 16 * NV results.  Every thread must call.
 // The shared buffer holds NRED values per (warp, column); longer vectors go
 // through it in blocks of NRED.
@@ -268,7 +244,7 @@ __device__ __forceinline__ void col_reduce(double (&v)[NV], double (*s_red)[16][
             int cc = o / nb, m = o % nb;
             double s = 0;
 #pragma unroll
-            for (int w = 0; w < 8; w++) s += s_red[w][cc][m];
+            for (int w = 0; w < TILE_WARPS; w++) s += s_red[w][cc][m];
             emit(cc, n0 + m, s);
         }
         __syncthreads();
@@ -279,14 +255,17 @@ __device__ __forceinline__ void col_reduce(double (&v)[NV], double (*s_red)[16][
 // k only (all of them by default).  Every J/K target is linear in the quartet
 // block, so launches over disjoint fk ranges add up to the whole class; a
 // class too large for one thread's registers runs as a few such launches.
-// CTAs per SM the register budget of jk_tile is sized for: small blocks
-// gain occupancy from a tighter budget, large ones need every register
+// 128-thread CTAs per SM the register budget of jk_tile is sized for: the
+// tightest budget under which ptxas keeps the class free of spills (80, 96,
+// 128, 168 and 255 registers; measured with -Xptxas -v on sm_100a: tighter
+// budgets spilled up to kilobytes per thread into local memory, whose L1
+// traffic then bounded the small classes)
 __host__ __device__ constexpr int tile_minb(int nf) {
-    return nf <= 3 ? 4 : (nf <= 9 ? 3 : (nf <= 27 ? 2 : 1));
+    return nf <= 3 ? 6 : (nf <= 6 ? 5 : (nf <= 10 ? 4 : (nf <= 27 ? 3 : 2)));
 }
 
 template <int LI, int LJ, int LK, int LL, typename F, int K0 = 0, int KN = ncart(LK)>
-__global__ void __launch_bounds__(256, tile_minb(ncart(LI) * ncart(LJ) * KN * ncart(LL)))
+__global__ void __launch_bounds__(TILE_THREADS, tile_minb(ncart(LI) * ncart(LJ) * KN * ncart(LL)))
 jk_tile(JKArgs A, JKTask T) {
     static_assert(K0 >= 0 && KN >= 1 && K0 + KN <= ncart(LK), "ket component range");
     // NFK: the components of shell k this launch evaluates, from K0 on
@@ -296,20 +275,21 @@ jk_tile(JKArgs A, JKTask T) {
     constexpr int GSZ = (LI + 1) * (LJ + 1) * (LK + 1) * (LL + 1);
     // column-reduction buffer: at most 32 values per (warp, column), 32 KB
     constexpr int NRED = imin(32, imax(NKL, imax(NFI * NFL, NFI * NFK)));
-    __shared__ double s_red[8][16][NRED];
+    __shared__ double s_red[TILE_WARPS][16][NRED];
 
-    // tile of this block
+    // half tile vb: bra pairs [a_begin, a_end) x ket pairs [b_begin, b_end)
+    auto half_tile = [&](const int vb) {
     int r, c;
-    tile_of_block(T, r, c);
+    tile_of_block(T, vb >> 1, r, c);
     const int ta = T.rows_are_b ? c : r, tb = T.rows_are_b ? r : c;
-    const int a_begin = T.a0 + ta * TILE, b_begin = T.b0 + tb * TILE;
-    const int a_end = min(T.a0 + T.na, a_begin + TILE), b_end = min(T.b0 + T.nb, b_begin + TILE);
-    if (T.diag && b_begin > a_end - 1) return;
+    const int a_begin = T.a0 + ta * TILE + (vb & 1) * TILE_ROWS, b_begin = T.b0 + tb * TILE;
+    const int a_end = min(T.a0 + T.na, a_begin + TILE_ROWS), b_end = min(T.b0 + T.nb, b_begin + TILE);
+    if (a_begin >= a_end || (T.diag && b_begin > a_end - 1)) return;
 
     const int row = threadIdx.x >> 4, col = threadIdx.x & 15;
     const int a = a_begin + row, b = b_begin + col;
     const bool row_ok = a < a_end, col_ok = b < b_end;
-    // shells shared across the tile
+    // shells shared across the half tile
     const int i_tile = __ldg(A.pair_bra + a_begin), k_tile = __ldg(A.pair_bra + b_begin);
     const int ish = row_ok ? __ldg(A.pair_bra + a) : i_tile;
     const int ksh = col_ok ? __ldg(A.pair_bra + b) : k_tile;
@@ -328,12 +308,6 @@ jk_tile(JKArgs A, JKTask T) {
         }
     }
     if (!__syncthreads_or(active)) return;
-
-    // the first density's blocks are copied while the integrals are evaluated
-    using R = DmRecord<NFI, NFJ, NFK, NFL>;
-    extern __shared__ double s_dm[];
-    double *rec = s_dm + threadIdx.x * R::STRIDE;
-    if (active && A.eri == nullptr) R::stage(rec, A.dm, A.nao, Q.i0, Q.j0, Q.k0, Q.l0);
 
     F acc[NF];
 #pragma unroll
@@ -413,10 +387,8 @@ jk_tile(JKArgs A, JKTask T) {
     const int i0t = __ldg(A.ao_loc + i_tile), k0t = __ldg(A.ao_loc + k_tile) + K0;
 #define ACC(fi, fj, fk, fl) ((double)acc[(((fi) * NFJ + (fj)) * NFK + (fk)) * NFL + (fl)])
     for (int id = 0; id < A.n_dm; id++) {
-        // density blocks of this quartet: staged for the first density at the
-        // start of the kernel, fetched here for the others
-        if (id > 0 && active) R::stage(rec, A.dm + id * nn, nao, Q.i0, Q.j0, Q.k0, Q.l0);
-        cp_async_wait_all();
+        const double *__restrict__ D = A.dm + id * nn;
+        auto ld = [&](int r0, int c0) { return __ldg(D + (size_t)r0 * nao + c0); };
         if (A.vj != nullptr) {
             double *VJ = A.vj + id * nn;
             double pij[NIJ];
@@ -425,7 +397,7 @@ jk_tile(JKArgs A, JKTask T) {
             if (active) {
 #pragma unroll
                 for (int kl = 0; kl < NKL; kl++) {
-                    const double d = rec[R::KL + kl];
+                    const double d = ld(Q.k0 + kl / NFL, Q.l0 + kl % NFL);
 #pragma unroll
                     for (int ij = 0; ij < NIJ; ij++) pij[ij] += (double)acc[ij * NKL + kl] * d;
                 }
@@ -444,7 +416,7 @@ jk_tile(JKArgs A, JKTask T) {
             if (active) {
 #pragma unroll
                 for (int ij = 0; ij < NIJ; ij++) {
-                    const double d = rec[R::IJ + ij];
+                    const double d = ld(Q.i0 + ij / NFJ, Q.j0 + ij % NFJ);
 #pragma unroll
                     for (int kl = 0; kl < NKL; kl++) pkl[kl] += (double)acc[ij * NKL + kl] * d;
                 }
@@ -469,7 +441,7 @@ jk_tile(JKArgs A, JKTask T) {
                 for (int fi = 0; fi < NFI; fi++)
 #pragma unroll
                     for (int fk = 0; fk < NFK; fk++) {
-                        const double d = rec[R::IK + fi * NFK + fk];
+                        const double d = ld(Q.i0 + fi, Q.k0 + fk);
 #pragma unroll
                         for (int fj = 0; fj < NFJ; fj++)
 #pragma unroll
@@ -489,7 +461,7 @@ jk_tile(JKArgs A, JKTask T) {
                     for (int fi = 0; fi < NFI; fi++)
 #pragma unroll
                         for (int fl = 0; fl < NFL; fl++) {
-                            const double d = rec[R::IL + fi * NFL + fl];
+                            const double d = ld(Q.i0 + fi, Q.l0 + fl);
 #pragma unroll
                             for (int fj = 0; fj < NFJ; fj++)
 #pragma unroll
@@ -520,7 +492,7 @@ jk_tile(JKArgs A, JKTask T) {
                     for (int fj = 0; fj < NFJ; fj++)
 #pragma unroll
                         for (int fk = 0; fk < NFK; fk++) {
-                            const double d = rec[R::JK + fj * NFK + fk];
+                            const double d = ld(Q.j0 + fj, Q.k0 + fk);
 #pragma unroll
                             for (int fi = 0; fi < NFI; fi++)
 #pragma unroll
@@ -551,7 +523,7 @@ jk_tile(JKArgs A, JKTask T) {
                     for (int fj = 0; fj < NFJ; fj++)
 #pragma unroll
                         for (int fl = 0; fl < NFL; fl++) {
-                            const double d = rec[R::JL + fj * NFL + fl];
+                            const double d = ld(Q.j0 + fj, Q.l0 + fl);
 #pragma unroll
                             for (int fi = 0; fi < NFI; fi++)
 #pragma unroll
@@ -562,7 +534,7 @@ jk_tile(JKArgs A, JKTask T) {
                     row_reduce(pik);
                     col_reduce<NFI * NFK, NRED>(pik, s_red, [&](int cc, int n, double v) {
                         // after the row sums each column holds its row total, so
-                        // column 0 carries the sum over the whole tile
+                        // column 0 carries the sum over the whole CTA
                         if (cc == 0 && v != 0)
                             atomicAdd(VK + (size_t)(i0t + n / NFK) * nao + k0t + n % NFK, v);
                     });
@@ -591,6 +563,16 @@ jk_tile(JKArgs A, JKTask T) {
         }
     }
 #undef ACC
+    };
+    if (T.ntiles_dev == nullptr) {
+        half_tile(blockIdx.x);
+        return;
+    }
+    const int nvb = 2 * __ldg(T.ntiles_dev);
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        half_tile(vb);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -644,8 +626,9 @@ jk_group(JKArgs A, JKTask T) {
     extern __shared__ double smem[];
     __shared__ int s_list[TILE * TILE];
     __shared__ int s_count;
+    auto tile = [&](const int x) {
     int a_begin, b_begin, count;
-    if (!tile_screen(A, T, s_list, &s_count, a_begin, b_begin, count)) return;
+    if (!tile_screen(A, T, x, s_list, &s_count, a_begin, b_begin, count)) return;
 
     const int g = threadIdx.x / TPQ;
     const int lane = threadIdx.x % TPQ;
@@ -918,6 +901,16 @@ jk_group(JKArgs A, JKTask T) {
             }
         }
     }
+    };
+    if (T.ntiles_dev == nullptr) {
+        tile(blockIdx.x);
+        return;
+    }
+    const int ntiles = __ldg(T.ntiles_dev);
+    for (int x = blockIdx.x; x < ntiles; x += gridDim.x) {
+        tile(x);
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -944,18 +937,9 @@ static int smem_attr(int bytes) {
     return 0;
 }
 
-// dynamic shared memory of a jk_tile launch: one density record per thread
-template <int LI, int LJ, int LK, int LL, int KN>
-constexpr int tile_smem() {
-    return 256 * DmRecord<ncart(LI), ncart(LJ), KN, ncart(LL)>::STRIDE * (int)sizeof(double);
-}
-
 template <int LI, int LJ, int LK, int LL, typename F, int K0, int KN>
 static int launch_tile_range(const JKArgs &args, const JKTask &task, int ntiles, cudaStream_t stream) {
-    constexpr int SMEM = tile_smem<LI, LJ, LK, LL, KN>();
-    static_assert(SMEM <= 200 * 1024, "density records per CTA");
-    if (smem_attr<jk_tile<LI, LJ, LK, LL, F, K0, KN>>(SMEM)) return 1;
-    jk_tile<LI, LJ, LK, LL, F, K0, KN><<<ntiles, 256, SMEM, stream>>>(args, task);
+    jk_tile<LI, LJ, LK, LL, F, K0, KN><<<bqc_grid(task, ntiles, 2, 16), TILE_THREADS, 0, stream>>>(args, task);
     return 0;
 }
 
@@ -996,7 +980,7 @@ static int launch_group_f(const JKArgs &args, const JKTask &task, cudaStream_t s
     int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
     if (ntiles == 0) return 0;
     if (smem_attr<jk_group<LI, LJ, LK, LL, NSPLIT, F>>((int)C::SMEM)) return 1;
-    jk_group<LI, LJ, LK, LL, NSPLIT, F><<<ntiles, C::NT, C::SMEM, stream>>>(args, task);
+    jk_group<LI, LJ, LK, LL, NSPLIT, F><<<bqc_grid(task, ntiles, 1, 8), C::NT, C::SMEM, stream>>>(args, task);
     return 0;
 }
 

@@ -157,3 +157,25 @@ def sto3g_like(elements):
                         _shell(0, ev, [_fit(0, ev, 2, zv)]),
                         _shell(1, ev, [_fit(1, ev, 2, zv)])]
     return out
+
+
+def synthetic_aux_basis(elements):
+    """A synthetic auxiliary (density-fitting) basis: uncontracted
+    even-tempered shells per element, s-f on heavy atoms and s-d on H, the
+    kind of shell structure JK-fitting sets have.  Generated here, not
+    copied from any published set; for the 3-centre integral engine and its
+    tests only."""
+    out = {}
+    for sym in elements:
+        if sym == 'H':
+            spec = [(0, 12., 3.5, 4), (1, 2.0, 3.0, 2), (2, 1.2, 1., 1)]
+        else:
+            Z = {'C': 6, 'N': 7, 'O': 8}[sym]
+            spec = [(0, 60. * Z, 3.2, 7), (1, 8. * Z, 3.0, 4), (2, 2.5 * Z, 2.8, 3),
+                    (3, 0.6 * Z, 2.5, 2)]
+        shells = []
+        for l, amax, ratio, n in spec:
+            for e in _even_tempered(amax, ratio, n):
+                shells.append([l, [e, 1.]])
+        out[sym] = shells
+    return out

@@ -18,7 +18,8 @@ SYMBOLS = ('GINTinit_basis_prod_cpu', 'GINTinit_basis_prod_gpu', 'GINTdel_basis_
            'GINTbuild_jk', 'GINTfill_int2e', 'BQCbuild_jk', 'BQCbuild_jk_mol', 'BQCbuild_jk_class', 'BQCcount_quartets',
            'BQCfp64_fma_peak', 'BQCdm_cond', 'BQCschwarz', 'BQCint1e', 'BQClaunch_counter',
            'BQCbuild_jk_noalloc', 'BQCmlp_linear_fwd', 'BQCmlp_linear_bwd', 'BQCmlp_adam',
-           'BQCmlp_to_bf16', 'BQCset_class_variant', 'BQCversion')
+           'BQCmlp_to_bf16', 'BQCset_class_variant', 'BQCversion', 'BQCplan_create',
+           'BQCplan_destroy', 'BQCbuild_jk_plan')
 
 
 def load_library(name='libbyteqc_b200'):
@@ -46,6 +47,13 @@ def load_library(name='libbyteqc_b200'):
         [ctypes.c_void_p] * 3 + [ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                                  ctypes.c_void_p]
     lib.BQCbuild_jk_noalloc.restype = ctypes.c_int
+    lib.BQCplan_create.restype = ctypes.c_int
+    lib.BQCplan_create.argtypes = [ctypes.c_void_p] * 4
+    lib.BQCplan_destroy.restype = None
+    lib.BQCplan_destroy.argtypes = [ctypes.c_void_p]
+    lib.BQCbuild_jk_plan.restype = ctypes.c_int
+    lib.BQCbuild_jk_plan.argtypes = [ctypes.c_void_p] * 6 + [ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                                              ctypes.c_double, ctypes.c_void_p]
     lib.BQCbuild_jk_mol.restype = ctypes.c_int
     lib.BQCbuild_jk_mol.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_double] + \
         [ctypes.c_void_p] * 3 + [ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double,

@@ -17,7 +17,8 @@ import torch
 
 from .. import lib as _libmod
 from ..gto import mole as gto
-from .hf import _VHFOpt, _dev, _ptr, _stream, basis_seg_contraction, _tile_order, PAIR_TILE
+from .hf import (_VHFOpt, _dev, _ptr, _stream, basis_seg_contraction, _tile_order, PAIR_TILE,
+                 free_basis_cache, make_plan)
 from .guess import atomic_density
 
 
@@ -132,7 +133,22 @@ class BatchedVHFOpt:
         self._bp_cpu, self._bp_gpu, self._mem, self._keep = helper._init_cache(
             self.bas_pair2shls, self.bas_pairs_locs, ncp, 0.5, self.pair_dummy)
         self.pair_q = torch.as_tensor(self.pair_q_host, device=_dev())
+        self._plan = make_plan(self._bp_gpu, self.pair_q_host, self.pair_mol_host)
         return self
+
+    def clear(self):
+        if getattr(self, '_plan', None):
+            _libmod.load_library().BQCplan_destroy(self._plan)
+            self._plan = None
+        if getattr(self, '_bp_cpu', None) is not None:
+            free_basis_cache(self._bp_cpu, self._bp_gpu)
+            self._bp_cpu = self._bp_gpu = None
+
+    def __del__(self):
+        try:
+            self.clear()
+        except Exception:
+            pass
 
     def jk_cart(self, dmc, tol=None, fp32_below=0.):
         """J', K' of the block-diagonal Cartesian density dmc (1, n, n)."""
@@ -146,14 +162,13 @@ class BatchedVHFOpt:
             raise RuntimeError('BQCdm_cond failed (%d)' % err)
         vj = torch.zeros_like(dmc)
         vk = torch.zeros_like(dmc)
-        err = lib.BQCbuild_jk_mol(ctypes.cast(self._bp_gpu, ctypes.c_void_p), _ptr(self.pair_q),
-                                  self.pair_q_host.ctypes.data_as(ctypes.c_void_p),
-                                  self.pair_mol_host.ctypes.data_as(ctypes.c_void_p),
-                                  _ptr(dm_cond), float(dm_cond.max()), _ptr(vj), _ptr(vk),
-                                  _ptr(dmc), n, 1, self.direct_scf_tol if tol is None else tol,
-                                  fp32_below, None, _stream())
+        # device-scheduled over the (molecule, class pair, tile) work of the
+        # batch: no host round trip, so the build can be graph-captured
+        err = lib.BQCbuild_jk_plan(self._plan, _ptr(self.pair_q), _ptr(dm_cond), _ptr(vj), _ptr(vk),
+                                   _ptr(dmc), n, 1, self.direct_scf_tol if tol is None else tol,
+                                   fp32_below, _stream())
         if err:
-            raise RuntimeError('BQCbuild_jk_mol failed (%d)' % err)
+            raise RuntimeError('BQCbuild_jk_plan failed (%d)' % err)
         return vj, vk
 
 
@@ -162,6 +177,10 @@ class BatchedRHF:
     padded batched DIIS / eigensolver; SAD guess; incremental Fock builds.
     Converged molecules keep their Fock matrix (their density no longer
     changes, so the difference density screens their quartets out)."""
+
+    # replay the J/K build of each cycle (density transform, screening table,
+    # device-scheduled build, back-transform) as one captured CUDA graph
+    use_graph = True
 
     def __init__(self, mols):
         self.mols = mols
@@ -239,6 +258,8 @@ class BatchedRHF:
             return Ct @ J @ C, Ct @ K @ C
 
         vj, vk = jk(D)
+        if self.use_graph:
+            jk = _graphed(jk, D)
         e_last = None
         done = torch.zeros(B, dtype=torch.bool, device=dev)
         focks, errs = [], []
@@ -291,6 +312,30 @@ class BatchedRHF:
         self.timings['jk'] = t_jk
         self.timings['total'] = time.perf_counter() - t0
         return self.e_tot
+
+
+def _graphed(fn, example):
+    """fn(x) -> (J, K) captured once as a CUDA graph over a static input
+    shaped like example; the returned function copies its argument in,
+    replays the graph and returns copies of the outputs.  The library's
+    launches all go to torch's current stream, which is the capture stream
+    inside torch.cuda.graph."""
+    static_in = example.clone()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        fn(static_in)                      # warm-up outside the capture
+    torch.cuda.current_stream().wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        static_out = fn(static_in)
+
+    def replay(x):
+        static_in.copy_(x)
+        graph.replay()
+        return static_out[0].clone(), static_out[1].clone()
+    replay.graph = graph
+    return replay
 
 
 def batch_systems(nmol, kmin=1, kmax=12, seed=0):

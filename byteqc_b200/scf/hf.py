@@ -198,6 +198,111 @@ def _tile_order(bra, ket, q, layout='q'):
     return out_b, out_k, out_q, dummy
 
 
+def schwarz_factors(mol, pair_lists, diag_fac):
+    """Schwarz factors sqrt(max |(ij|ij)|) of every pair of the given lists,
+    one list (bra shells, ket shells) per class of pairs sharing
+    (l, nprim) on each side, computed on the device (BQCschwarz); the e12
+    diagonal factor diag_fac is undone.  Returns one array per list."""
+    lib = _libmod.load_library()
+    ncptype = len(pair_lists)
+    locs = np.append(0, np.cumsum([len(x[0]) for x in pair_lists])).astype(np.int32)
+    p2s = np.vstack([np.hstack([x[0] for x in pair_lists]),
+                     np.hstack([x[1] for x in pair_lists])]).astype(np.int32)
+    bp_cpu, bp_gpu, mem, keep = basis_cache(mol, p2s, locs, ncptype, diag_fac)
+    q_all = torch.zeros(max(int(locs[-1]), 1), dtype=torch.float64, device=_dev())
+    for c in range(ncptype):
+        if locs[c + 1] > locs[c]:
+            err = lib.BQCschwarz(bp_gpu, ctypes.c_int(c), ctypes.c_double(diag_fac),
+                                 _ptr(q_all[locs[c]:]), _stream())
+            if err:
+                raise RuntimeError('BQCschwarz failed (%d)' % err)
+    q_all = q_all.cpu().numpy()
+    free_basis_cache(bp_cpu, bp_gpu)
+    del mem, keep
+    return [q_all[locs[c]:locs[c + 1]] for c in range(ncptype)]
+
+
+def make_plan(bp_gpu, pair_q_host, pair_mol_host=None):
+    """The device schedule of J/K builds over a basis-product cache
+    (BQCplan_create); released with BQCplan_destroy before the cache."""
+    lib = _libmod.load_library()
+    plan = ctypes.c_void_p()
+    mol = pair_mol_host.ctypes.data_as(ctypes.c_void_p) if pair_mol_host is not None else None
+    err = lib.BQCplan_create(ctypes.cast(bp_gpu, ctypes.c_void_p),
+                             pair_q_host.ctypes.data_as(ctypes.c_void_p), mol, ctypes.byref(plan))
+    if err:
+        raise RuntimeError('BQCplan_create failed (%d)' % err)
+    return plan
+
+
+def free_basis_cache(bp_cpu, bp_gpu):
+    """Release both structs.  The device copy shares the host blocks of
+    the cpu cache, so deleting it frees them (cuobc/scf/hf.py:439-442
+    deletes only that copy); the cpu struct is then released with its
+    shared pointers cleared."""
+    lib = _libmod.load_library()
+    shared = bool(bp_gpu)
+    if shared:
+        lib.GINTdel_basis_prod(ctypes.byref(bp_gpu))
+    if bp_cpu:
+        if shared:
+            c = bp_cpu.contents
+            c.cptype = None
+            c.primitive_pairs_locs = None
+            c.aexyz = None
+        lib.GINTdel_basis_prod(ctypes.byref(bp_cpu))
+
+
+def basis_cache(mol, pair2shls, pairs_locs, ncptype, diag_fac, dummy=None):
+    """The basis-product cache of a pair list (GINTinit_basis_prod_cpu, then
+    GINTinit_basis_prod_gpu on device copies of ao_loc, shell coordinates,
+    primitive-pair block and pair list, as cuobc/scf/hf.py:410-437).  Pairs
+    flagged in dummy get e12 = 0.  Returns (cpu cache, device cache, device
+    buffers, host arrays the caches borrow)."""
+    lib = _libmod.load_library()
+    bp_cpu = ctypes.POINTER(_libmod.BasisProdCache)()
+    bas_coords = np.empty(mol.nbas * 3)
+    pair2shls = np.ascontiguousarray(pair2shls, dtype=np.int32)
+    pairs_locs = np.ascontiguousarray(pairs_locs, dtype=np.int32)
+    atm = np.ascontiguousarray(mol._atm, dtype=np.int32)
+    bas = np.ascontiguousarray(mol._bas, dtype=np.int32)
+    env = np.ascontiguousarray(mol._env)
+    lib.GINTinit_basis_prod_cpu(
+        ctypes.byref(bp_cpu), ctypes.c_double(diag_fac),
+        bas_coords.ctypes.data_as(ctypes.c_void_p),
+        pair2shls.ctypes.data_as(ctypes.c_void_p), pairs_locs.ctypes.data_as(ctypes.c_void_p),
+        ctypes.c_int(ncptype), atm.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(mol.natm),
+        bas.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(mol.nbas),
+        env.ctypes.data_as(ctypes.c_void_p))
+    nprim = bp_cpu.contents.primitive_pairs_locs[ncptype]
+    aexyz = np.ctypeslib.as_array(bp_cpu.contents.aexyz, (max(nprim, 1) * 5,)).copy()
+    if dummy is not None and dummy.any():
+        # padding pairs contribute exactly zero: e12 = 0 for all their primitives
+        e12 = aexyz[nprim:2 * nprim]
+        for c in range(ncptype):
+            p0, p1 = pairs_locs[c], pairs_locs[c + 1]
+            d = np.flatnonzero(dummy[p0:p1])
+            if len(d):
+                n12 = bp_cpu.contents.cptype[c].nprim_12
+                base = bp_cpu.contents.primitive_pairs_locs[c]
+                idx = (base + d[:, None] * n12 + np.arange(n12)[None, :]).ravel()
+                e12[idx] = 0.
+    dev = _dev()
+    mem = {
+        'ao_loc': torch.as_tensor(mol.ao_loc_nr(cart=True), dtype=torch.int32, device=dev),
+        'bas_coords': torch.as_tensor(bas_coords, device=dev),
+        'aexyz': torch.as_tensor(aexyz, device=dev),
+        'pair2shls': torch.as_tensor(pair2shls.ravel(), device=dev),
+    }
+    bp_gpu = ctypes.POINTER(_libmod.BasisProdCache)()
+    lib.GINTinit_basis_prod_gpu(ctypes.byref(bp_cpu), ctypes.byref(bp_gpu),
+                                _ptr(mem['ao_loc']), _ptr(mem['bas_coords']),
+                                _ptr(mem['aexyz']), _ptr(mem['pair2shls']))
+    # keep host arrays alive: the cache borrows them
+    keep = (pair2shls, pairs_locs, atm, bas, env)
+    return bp_cpu, bp_gpu, mem, keep
+
+
 class _VHFOpt:
     """Basis sort, Schwarz pair lists and the device basis-product cache.
 
@@ -221,66 +326,10 @@ class _VHFOpt:
 
     # -- helpers ---------------------------------------------------------------
     def _init_cache(self, pair2shls, pairs_locs, ncptype, diag_fac, dummy=None):
-        lib = _libmod.load_library()
-        mol = self.mol
-        bp_cpu = ctypes.POINTER(_libmod.BasisProdCache)()
-        bas_coords = np.empty(mol.nbas * 3)
-        pair2shls = np.ascontiguousarray(pair2shls, dtype=np.int32)
-        pairs_locs = np.ascontiguousarray(pairs_locs, dtype=np.int32)
-        atm = np.ascontiguousarray(mol._atm, dtype=np.int32)
-        bas = np.ascontiguousarray(mol._bas, dtype=np.int32)
-        env = np.ascontiguousarray(mol._env)
-        lib.GINTinit_basis_prod_cpu(
-            ctypes.byref(bp_cpu), ctypes.c_double(diag_fac),
-            bas_coords.ctypes.data_as(ctypes.c_void_p),
-            pair2shls.ctypes.data_as(ctypes.c_void_p), pairs_locs.ctypes.data_as(ctypes.c_void_p),
-            ctypes.c_int(ncptype), atm.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(mol.natm),
-            bas.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(mol.nbas),
-            env.ctypes.data_as(ctypes.c_void_p))
-        nprim = bp_cpu.contents.primitive_pairs_locs[ncptype]
-        aexyz = np.ctypeslib.as_array(bp_cpu.contents.aexyz, (max(nprim, 1) * 5,)).copy()
-        if dummy is not None and dummy.any():
-            # padding pairs contribute exactly zero: e12 = 0 for all their primitives
-            e12 = aexyz[nprim:2 * nprim]
-            for c in range(ncptype):
-                p0, p1 = pairs_locs[c], pairs_locs[c + 1]
-                d = np.flatnonzero(dummy[p0:p1])
-                if len(d):
-                    n12 = bp_cpu.contents.cptype[c].nprim_12
-                    base = bp_cpu.contents.primitive_pairs_locs[c]
-                    idx = (base + d[:, None] * n12 + np.arange(n12)[None, :]).ravel()
-                    e12[idx] = 0.
-        dev = _dev()
-        mem = {
-            'ao_loc': torch.as_tensor(mol.ao_loc_nr(cart=True), dtype=torch.int32, device=dev),
-            'bas_coords': torch.as_tensor(bas_coords, device=dev),
-            'aexyz': torch.as_tensor(aexyz, device=dev),
-            'pair2shls': torch.as_tensor(pair2shls.ravel(), device=dev),
-        }
-        bp_gpu = ctypes.POINTER(_libmod.BasisProdCache)()
-        lib.GINTinit_basis_prod_gpu(ctypes.byref(bp_cpu), ctypes.byref(bp_gpu),
-                                    _ptr(mem['ao_loc']), _ptr(mem['bas_coords']),
-                                    _ptr(mem['aexyz']), _ptr(mem['pair2shls']))
-        # keep host arrays alive: the cache borrows them
-        keep = (pair2shls, pairs_locs, atm, bas, env)
-        return bp_cpu, bp_gpu, mem, keep
+        return basis_cache(self.mol, pair2shls, pairs_locs, ncptype, diag_fac, dummy)
 
     def _free_cache(self, bp_cpu, bp_gpu):
-        """Release both structs.  The device copy shares the host blocks of
-        the cpu cache, so deleting it frees them (cuobc/scf/hf.py:439-442
-        deletes only that copy); the cpu struct is then released with its
-        shared pointers cleared."""
-        lib = _libmod.load_library()
-        shared = bool(bp_gpu)
-        if shared:
-            lib.GINTdel_basis_prod(ctypes.byref(bp_gpu))
-        if bp_cpu:
-            if shared:
-                c = bp_cpu.contents
-                c.cptype = None
-                c.primitive_pairs_locs = None
-                c.aexyz = None
-            lib.GINTdel_basis_prod(ctypes.byref(bp_cpu))
+        free_basis_cache(bp_cpu, bp_gpu)
 
     # -- build -----------------------------------------------------------------
     def build(self, cutoff=1e-13, group_size=None, diag_block_with_triu=False, gpus=None):
@@ -315,29 +364,17 @@ class _VHFOpt:
                     m = i >= j
                     i, j = i[m], j[m]
                 pair_lists.append((i, j))
-        ncptype = len(pair_lists)
-        locs = np.append(0, np.cumsum([len(x[0]) for x in pair_lists])).astype(np.int32)
-        p2s = np.vstack([np.hstack([x[0] for x in pair_lists]),
-                         np.hstack([x[1] for x in pair_lists])]).astype(np.int32)
-        bp_cpu, bp_gpu, mem, keep = self._init_cache(p2s, locs, ncptype, scale_diag)
-        q_all = torch.zeros(max(locs[-1], 1), dtype=torch.float64, device=_dev())
-        for c in range(ncptype):
-            if locs[c + 1] > locs[c]:
-                err = lib.BQCschwarz(bp_gpu, ctypes.c_int(c), ctypes.c_double(scale_diag),
-                                     _ptr(q_all[locs[c]:]), _stream())
-                if err:
-                    raise RuntimeError('BQCschwarz failed (%d)' % err)
-        q_all = q_all.cpu().numpy()
-        self._free_cache(bp_cpu, bp_gpu)
-        del mem, keep
+        q_all = schwarz_factors(mol, pair_lists, scale_diag)
 
         # pass 2: keep q > cutoff and lay every class out in tiles of 16 pairs
         # (see _tile_order)
+        ncptype = len(pair_lists)
         pair2bra, pair2ket, qs, log_qs, dummies = [], [], [], [], []
         for c in range(ncptype):
-            q = q_all[locs[c]:locs[c + 1]]
+            b, k = pair_lists[c]
+            q = q_all[c]
             keep = q > cutoff
-            b, k, q = p2s[0, locs[c]:locs[c + 1]][keep], p2s[1, locs[c]:locs[c + 1]][keep], q[keep]
+            b, k, q = b[keep].astype(np.int32), k[keep].astype(np.int32), q[keep]
             b, k, q, dummy = _tile_order(b, k, q, self.tile_layout)
             pair2bra.append(b)
             pair2ket.append(k)
@@ -360,6 +397,7 @@ class _VHFOpt:
         self.cptype = [(self._bp_cpu.contents.cptype[c].l_bra, self._bp_cpu.contents.cptype[c].l_ket,
                         self._bp_cpu.contents.cptype[c].nprim_12,
                         self._bp_cpu.contents.cptype[c].npairs) for c in range(ncptype)]
+        self._plan = make_plan(self._bp_gpu, self.pair_q_host)
         return self
 
     @property
@@ -367,6 +405,9 @@ class _VHFOpt:
         return self._bp_gpu
 
     def clear(self):
+        if getattr(self, '_plan', None):
+            _libmod.load_library().BQCplan_destroy(self._plan)
+            self._plan = None
         if self._bp_cpu is not None:
             self._free_cache(self._bp_cpu, self._bp_gpu)
             self._bp_cpu = self._bp_gpu = None
@@ -398,15 +439,11 @@ class _VHFOpt:
         vj = torch.zeros_like(dmc) if with_j else None
         vk = torch.zeros_like(dmc) if with_k else None
         tol = self.direct_scf_tol if tol is None else tol
-        dm_max = float(dm_cond.max())
-        err = lib.BQCbuild_jk(ctypes.cast(self._bp_gpu, ctypes.c_void_p), _ptr(self.pair_q),
-                              self.pair_q_host.ctypes.data_as(ctypes.c_void_p), _ptr(dm_cond),
-                              ctypes.c_double(dm_max), _ptr(vj), _ptr(vk),
-                              _ptr(dmc), ctypes.c_int(nao), ctypes.c_int(n_dm),
-                              ctypes.c_double(tol), ctypes.c_double(fp32_below),
-                              ctypes.c_void_p(0), _stream())
+        # the device-scheduled build: no host round trip, no allocation
+        err = lib.BQCbuild_jk_plan(self._plan, _ptr(self.pair_q), _ptr(dm_cond), _ptr(vj), _ptr(vk),
+                                   _ptr(dmc), nao, n_dm, tol, fp32_below, _stream())
         if err:
-            raise RuntimeError('BQCbuild_jk failed (%d)' % err)
+            raise RuntimeError('BQCbuild_jk_plan failed (%d)' % err)
         if vj is not None:
             vj = 2. * (vj + vj.transpose(-1, -2))
         if vk is not None:

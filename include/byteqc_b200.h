@@ -179,6 +179,29 @@ int BQCbuild_jk_noalloc(const BasisProdCache *bpcache, const double *pair_q, dou
                         double *vk, const double *dm, int nao, int n_dm, double tol,
                         cudaStream_t stream);
 
+/* ---- device-scheduled builds ----------------------------------------------
+ * No reference counterpart (the reference prunes the quartet tiles on the
+ * host and launches one kernel per class pair and log-q bin,
+ * cuobc/scf/hf.py:111-166, cuobc/lib/gvhf/nr_jk_driver.cu:252-280).
+ *
+ * A plan is created once per basis-product cache (device copy, kept alive by
+ * the caller) from the host Schwarz factors of its pair list (pair_q_host,
+ * descending within each tile of 16 pairs and along the tiles' first
+ * pairs; pair_mol_host: the molecule of every pair for batched molecules,
+ * else NULL).  BQCbuild_jk_plan then computes dm_max, the surviving 16 x 16
+ * tiles of every class pair and their offsets on the device and launches
+ * fixed grids that stride over them: no host work, no allocation and the
+ * same launches every build, so a build can be captured in a CUDA graph.
+ * Its results equal BQCbuild_jk's with the same arguments.  Returns 0, 1 on
+ * a CUDA error, 2 for l > 3, 3 for missing arguments. */
+typedef struct BQCPlan BQCPlan;
+int BQCplan_create(const BasisProdCache *bpcache, const double *pair_q_host,
+                   const int *pair_mol_host, BQCPlan **plan);
+void BQCplan_destroy(BQCPlan *plan);
+int BQCbuild_jk_plan(const BQCPlan *plan, const double *pair_q, const double *dm_cond, double *vj,
+                     double *vk, const double *dm, int nao, int n_dm, double tol,
+                     double fp32_below, cudaStream_t stream);
+
 /* ---- learned initial density: BF16 tensor-core MLP kernels ----------------
  * No reference counterpart (the reference starts from pyscf's minao guess).
  * Row-major X (M x K, BF16), W (N x K, BF16); M, N, K multiples of 16

@@ -315,3 +315,45 @@ def test_fill_int2e_matches_oracle(cuda, kind):
     # a missing output buffer is an argument error
     assert lib.GINTfill_int2e(ctypes.cast(opt.bpcache, ctypes.c_void_p), None, n, vp(strides),
                               vp(offs), vp(bi), vp(bk), 1, 0, 0, _stream()) == 3
+
+
+@pytest.mark.parametrize('fp32_below', [0., 1e-6])
+def test_device_schedule_matches_host_pruning(cuda, fp32_below):
+    """BQCbuild_jk_plan (tiles pruned and counted on the device, persistent
+    launches) gives the J/K of BQCbuild_jk (tiles pruned on the host) for
+    two densities at once, with and without the FP32 band."""
+    import ctypes
+    import torch
+    from byteqc_b200 import lib as L
+    from byteqc_b200.scf import hf
+    from byteqc_b200.scf.hf import _ptr, _stream
+    lib = L.load_library()
+    mol = _mol('cc-pvtz', nw=3, seed=12)
+    opt = hf._VHFOpt(mol).build()
+    rng = np.random.default_rng(3)
+    d = rng.random((2, mol.nao, mol.nao)) * 1e-2
+    C = opt.coeff_dev
+    dmc = (C @ torch.as_tensor(d + d.transpose(0, 2, 1), device=cuda) @ C.T).contiguous()
+    nao = dmc.shape[-1]
+    dm_cond = torch.empty((opt.mol.nbas, opt.mol.nbas), dtype=torch.float64, device=cuda)
+    assert lib.BQCdm_cond(_ptr(dmc), 2, nao, _ptr(opt._mem['ao_loc']), opt.mol.nbas, _ptr(dm_cond),
+                          _stream()) == 0
+    out = []
+    for plan in (False, True):
+        vj = torch.zeros_like(dmc)
+        vk = torch.zeros_like(dmc)
+        if plan:
+            err = lib.BQCbuild_jk_plan(opt._plan, _ptr(opt.pair_q), _ptr(dm_cond), _ptr(vj), _ptr(vk),
+                                       _ptr(dmc), nao, 2, opt.direct_scf_tol, fp32_below, _stream())
+        else:
+            err = lib.BQCbuild_jk(ctypes.cast(opt.bpcache, ctypes.c_void_p), _ptr(opt.pair_q),
+                                  opt.pair_q_host.ctypes.data_as(ctypes.c_void_p), _ptr(dm_cond),
+                                  float(dm_cond.max()), _ptr(vj), _ptr(vk), _ptr(dmc), nao, 2,
+                                  opt.direct_scf_tol, fp32_below, None, _stream())
+        assert err == 0
+        out.append((vj, vk))
+    torch.cuda.synchronize()
+    (j0, k0), (j1, k1) = out
+    assert float((j1 - j0).abs().max()) < 1e-12 * max(1., float(j0.abs().max()))
+    assert float((k1 - k0).abs().max()) < 1e-12 * max(1., float(k0.abs().max()))
+    assert float(j0.abs().max()) > 0

@@ -88,3 +88,36 @@ def test_rhf_water_is_variational():
     S, _, _ = oracle.int1e(mol)
     assert abs(np.sum(dm * S) - 10) < 1e-8
     assert -76.5 < e < -74.5
+
+
+def test_oracle_three_centre_closed_form():
+    """The constant s shell of the density-fitting path (exponent 0, the
+    s-function factor cancelled) turns the oracle's four-centre quartet
+    (a b | c 1) into the three-centre Coulomb integral, whose closed form for
+    normalised s Gaussians is
+    Na Nb Nc exp(-ab/p |AB|^2) 2 pi^(5/2) / (p c sqrt(p + c)) F0(pc/(p+c) |PC|^2)."""
+    import math
+    from byteqc_b200.gto.mole import Mole
+    from byteqc_b200.df.int3c import make_fake_mol, conc_mol
+    from oracle import oracle
+    atoms = [('H', (0., 0., 0.)), ('H', (0.3, -0.4, 1.1)), ('H', (-0.7, 0.2, 0.5))]
+    exps = [1.3, 0.45, 2.2]
+    mol = Mole(atoms, {'H': [[0, [1., 1.]]]}, unit='Bohr')
+    env = list(mol._env)
+    for ish, a in enumerate(exps):     # one primitive s shell per atom, own exponent
+        mol._bas[ish, 5] = len(env)
+        mol._bas[ish, 6] = len(env) + 1
+        env += [a, (2 * a / math.pi) ** .75 / 0.282094791773878143]
+    mol._env = np.asarray(env)
+    tot = conc_mol(mol, make_fake_mol())
+    R = mol.atom_coords()
+    a, b, c = exps
+    p = a + b
+    P = (a * R[0] + b * R[1]) / p
+    T = p * c / (p + c) * float(np.sum((P - R[2]) ** 2))
+    F0 = math.sqrt(math.pi / (4 * T)) * math.erf(math.sqrt(T))
+    Ns = [(2 * e / math.pi) ** .75 for e in exps]
+    ref = Ns[0] * Ns[1] * Ns[2] * math.exp(-a * b / p * float(np.sum((R[0] - R[1]) ** 2))) * \
+        2 * math.pi ** 2.5 / (p * c * math.sqrt(p + c)) * F0
+    got = oracle.eri_shells(tot, 0, 1, 2, 3).ravel()[0]
+    assert abs(got - ref) < 1e-14 * abs(ref), (got, ref)
