@@ -50,6 +50,14 @@ def parse():
     p.add_argument('--basis', default='cc-pvtz')
     p.add_argument('--conv', type=float, default=1e-8)
     p.add_argument('--no-extras', action='store_true', help='skip e2e/roofline/cpu legs')
+    p.add_argument('--per-class', action='store_true',
+                   help='time one J/K build class by class (this engine, or with --impl '
+                        'reference the reference kernels) and print the per-class sums')
+    p.add_argument('--noscreen', action='store_true',
+                   help='with --per-class: every quartet of the pair lists, no screening')
+    p.add_argument('--only', default=None,
+                   help='with --per-class: only the class pairs of shape li,lj,lk,ll')
+    p.add_argument('--reps', type=int, default=2, help='with --per-class: builds timed')
     return p.parse_args()
 
 
@@ -130,7 +138,7 @@ def scf_once(mol, conv, host_loop=False, fast=False):
     if fast:
         mf.fp32_threshold = FP32_BELOW
         mf.early_tol = EARLY_TOL
-        if getattr(mol, 'basis_name', '') == 'cc-pvdz':
+        if has_learned_guess(mol):
             mf.init_guess = 'mlp'
     if host_loop:
         e = mf.kernel_hostloop()
@@ -138,6 +146,11 @@ def scf_once(mol, conv, host_loop=False, fast=False):
         e = mf.kernel()
     torch.cuda.synchronize()
     return mf, e
+
+
+def has_learned_guess(mol):
+    from byteqc_b200.learned.infer import weights_for
+    return weights_for(mol) is not None
 
 
 def roofline(mf, peak):
@@ -273,6 +286,10 @@ def main():
     world = int(os.environ.get('WORLD_SIZE', 1))
     local = int(os.environ.get('LOCAL_RANK', 0))
 
+    if args.per_class:
+        if rank == 0:
+            per_class(args)
+        return
     if args.impl == 'reference':
         if rank == 0:
             run_reference(args)
@@ -320,8 +337,9 @@ def main():
             'form': 'fast: incremental builds with FP32 for quartets with bound < %g and '
                     'screening at %g, then one full FP64 rebuild and FP64 incremental builds at '
                     '1e-13 to convergence%s' % (
-                        FP32_BELOW, EARLY_TOL, '; learned guess' if mol.basis_name == 'cc-pvdz' else
-                        '; SAD guess (the learned guess is trained for the cc-pVDZ shape)'),
+                        FP32_BELOW, EARLY_TOL, '; learned initial density (SAD fallback)'
+                        if has_learned_guess(mol) else
+                        '; SAD guess (no learned model for this basis shape)'),
             'config': config(args, mol), 'clocks': clk.summary(), 'gpu_launches': int(launches),
             'scf': {'energy': e, 'cycles': mf.cycles, 'converged': bool(mf.converged),
                     'jk_s': round(mf.timings.get('jk', 0), 3)}}
@@ -568,6 +586,103 @@ def run_reference(args):
         line['reference_gpu'] = {'unavailable': '%s: %s' % (type(exc).__name__, exc)}
     ref.close()
     print(json.dumps(line))
+
+
+def per_class(args):
+    """One J/K build of the workload on the jk.py density, class pair by class
+    pair (CUDA events on the launching stream), summed per class shape
+    li lj lk ll; the last of --reps builds is printed.  With --impl reference
+    the reference's kernels run over the pair lists of its own host logic
+    (oracle/ref_gpu.py), without the engine library; with --noscreen both
+    evaluate every quartet of their lists (no density screen, one bin)."""
+    import ctypes
+    import torch
+    torch.cuda.set_device(0)
+    mol = workload(args)
+    only = tuple(int(x) for x in args.only.split(',')) if args.only else None
+    rng = np.random.default_rng(2341)
+    dm = rng.random((mol.nao, mol.nao))
+    dm = torch.as_tensor(0.1 * (dm + dm.T), device='cuda')
+    res, tot = {}, 0.
+    if args.impl == 'reference':
+        from oracle import ref_gpu
+        opt = ref_gpu.RefVHFOpt(mol).build()
+        ref = ref_gpu.RefJK(opt)
+        C = torch.as_tensor(opt.coeff, device='cuda')
+        dmc = (C @ dm @ C.T)[None].contiguous()
+        tasks = ref.tasks(dmc)
+        nbins = ref.nbins
+        if args.noscreen:
+            nb = ref.pairs_locs[1:] - ref.pairs_locs[:-1]
+            tasks = [(i, j, np.array([0, nb[i]], np.int32), np.array([0, nb[j]], np.int32))
+                     for i in range(opt.ncptype) for j in range(i + 1) if nb[i] and nb[j]]
+            nbins = 1
+        lt = [(int(opt.uniq_l_ctr[p, 0]), int(opt.uniq_l_ctr[q, 0]))
+              for p in range(len(opt.uniq_l_ctr)) for q in range(p + 1)]
+        vj = torch.zeros_like(dmc)
+        vk = torch.zeros_like(dmc)
+        vp = lambda x: x.ctypes.data_as(ctypes.c_void_p)
+        tp = lambda t: ctypes.c_void_p(t.data_ptr())
+        stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+        jobs = []
+        for cij, ckl, bi, bk in tasks:
+            shape = lt[cij] + lt[ckl]
+            if only is None or shape in (only, only[2:] + only[:2]):
+                jobs.append((shape, lambda cij=cij, ckl=ckl, bi=bi, bk=bk: ref.lv.GINTbuild_jk(
+                    ref.bp_gpu, tp(vj), tp(vk), tp(dmc), ctypes.c_int(dmc.shape[-1]), ctypes.c_int(1),
+                    vp(bi), vp(bk), ctypes.c_int(nbins), ctypes.c_int(cij), ctypes.c_int(ckl), stream)))
+    else:
+        from byteqc_b200 import lib as L
+        from byteqc_b200.scf import hf
+        from byteqc_b200.scf.hf import _ptr, _stream
+        lib = L.load_library()
+        opt = hf._VHFOpt(mol).build()
+        C = opt.coeff_dev
+        dmc = (C @ dm @ C.T)[None].contiguous()
+        nao = dmc.shape[-1]
+        dm_cond = torch.empty((opt.mol.nbas, opt.mol.nbas), dtype=torch.float64, device='cuda')
+        lib.BQCdm_cond(_ptr(dmc), 1, nao, _ptr(opt._mem['ao_loc']), opt.mol.nbas, _ptr(dm_cond),
+                       _stream())
+        dm_max = float(dm_cond.max())
+        qh = opt.pair_q_host.ctypes.data_as(ctypes.c_void_p)
+        bp = ctypes.cast(opt.bpcache, ctypes.c_void_p)
+        vj = torch.zeros_like(dmc)
+        vk = torch.zeros_like(dmc)
+        jobs = []
+        for cij in range(opt.ncptype):
+            for ckl in range(cij + 1):
+                if opt.cptype[cij][3] == 0 or opt.cptype[ckl][3] == 0:
+                    continue
+                shape = tuple(opt.cptype[cij][:2]) + tuple(opt.cptype[ckl][:2])
+                if only is not None and shape not in (only, only[2:] + only[:2]):
+                    continue
+                if args.noscreen:
+                    fn = lambda cij=cij, ckl=ckl: lib.BQCbuild_jk_class(
+                        bp, cij, ckl, None, None, None, 1.0, _ptr(vj), _ptr(vk), _ptr(dmc), nao, 1,
+                        0., 0., None, _stream())
+                else:
+                    fn = lambda cij=cij, ckl=ckl: lib.BQCbuild_jk_class(
+                        bp, cij, ckl, _ptr(opt.pair_q), qh, _ptr(dm_cond), dm_max, _ptr(vj),
+                        _ptr(vk), _ptr(dmc), nao, 1, opt.direct_scf_tol, 0., None, _stream())
+                jobs.append((shape, fn))
+    for rep in range(args.reps):
+        res, tot = {}, 0.
+        for shape, fn in jobs:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            err = fn()
+            e1.record()
+            torch.cuda.synchronize()
+            if err:
+                raise RuntimeError('J/K build failed for class %s (%d)' % (shape, err))
+            ms = e0.elapsed_time(e1)
+            key = '(%s%s|%s%s)' % tuple('spdf'[x] for x in shape)
+            res[key] = res.get(key, 0.) + ms
+            tot += ms
+    print(json.dumps({'per_class': args.impl, 'workload': '(H2O)%d/%s-shaped' % (args.nwater, args.basis),
+                      'density': JKPY_DENSITY, 'screen': not args.noscreen, 'total_ms': round(tot, 2),
+                      'classes_ms': {k: round(v, 3) for k, v in sorted(res.items(), key=lambda x: -x[1])}}))
 
 
 def max_over_ranks(value, device):

@@ -46,7 +46,11 @@ def has_variants(li, lj, lk, ll):
     if n12 * n34 <= SMALL_NF:
         return False
     ck = SMALL_NF // (n12 * _nc(l4))
-    return ck >= 1 and -(-_nc(l3) // ck) <= MAX_SPLIT
+    if ck >= 1 and -(-_nc(l3) // ck) <= MAX_SPLIT:
+        return True
+    # an s-s ket: the bra's first shell splits with bra and ket exchanged
+    cks = SMALL_NF // (n34 * _nc(l2))
+    return ck == 0 and n34 == 1 and cks >= 1 and -(-_nc(l1) // cks) <= MAX_SPLIT
 
 
 def apply(choice):

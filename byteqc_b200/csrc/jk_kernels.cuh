@@ -255,13 +255,15 @@ __device__ __forceinline__ void col_reduce(double (&v)[NV], double (*s_red)[16][
 // k only (all of them by default).  Every J/K target is linear in the quartet
 // block, so launches over disjoint fk ranges add up to the whole class; a
 // class too large for one thread's registers runs as a few such launches.
-// 128-thread CTAs per SM the register budget of jk_tile is sized for: the
-// tightest budget under which ptxas keeps the class free of spills (80, 96,
-// 128, 168 and 255 registers; measured with -Xptxas -v on sm_100a: tighter
-// budgets spilled up to kilobytes per thread into local memory, whose L1
-// traffic then bounded the small classes)
+// 128-thread CTAs per SM the register budget of jk_tile is sized for (64,
+// 85, 128 and 255 registers): small blocks gain occupancy from a tight
+// budget, large ones need every register.  Measured on B200 against the
+// budgets under which ptxas spills nothing (80-168 registers for the blocks
+// of 3-27 components): those removed up to 13e9 local-memory sectors per
+// launch of the small classes but lost more to the lower occupancy
+// (a full (H2O)_64 / cc-pVTZ build 7 % slower).
 __host__ __device__ constexpr int tile_minb(int nf) {
-    return nf <= 3 ? 6 : (nf <= 6 ? 5 : (nf <= 10 ? 4 : (nf <= 27 ? 3 : 2)));
+    return nf <= 3 ? 8 : (nf <= 9 ? 6 : (nf <= 27 ? 4 : 2));
 }
 
 template <int LI, int LJ, int LK, int LL, typename F, int K0 = 0, int KN = ncart(LK)>
@@ -564,11 +566,9 @@ jk_tile(JKArgs A, JKTask T) {
     }
 #undef ACC
     };
-    if (T.ntiles_dev == nullptr) {
-        half_tile(blockIdx.x);
-        return;
-    }
-    const int nvb = 2 * __ldg(T.ntiles_dev);
+    // one call site, so the body is instantiated once: without a device tile
+    // count the grid is exactly the half tiles and the loop runs once
+    const int nvb = T.ntiles_dev == nullptr ? (int)gridDim.x : 2 * __ldg(T.ntiles_dev);
     for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
         half_tile(vb);
         __syncthreads();
@@ -902,11 +902,7 @@ jk_group(JKArgs A, JKTask T) {
         }
     }
     };
-    if (T.ntiles_dev == nullptr) {
-        tile(blockIdx.x);
-        return;
-    }
-    const int ntiles = __ldg(T.ntiles_dev);
+    const int ntiles = T.ntiles_dev == nullptr ? (int)gridDim.x : __ldg(T.ntiles_dev);
     for (int x = blockIdx.x; x < ntiles; x += gridDim.x) {
         tile(x);
         __syncthreads();
@@ -1016,16 +1012,26 @@ static int launch_class(const JKArgs &args, const JKTask &task, int fp32, cudaSt
             if (v == BQC_VARIANT_SPLIT || (v == BQC_VARIANT_AUTO && NCH <= SPLIT_AUTO))
                 return launch_split<L1, L2, L3, L4, CK>(args, task, fp32, stream);
         }
+        // the task with bra and ket exchanged (diag tasks have identical
+        // lists on both sides; the a >= b rule stays)
+        JKTask sw = task;
+        sw.a0 = task.b0; sw.na = task.nb; sw.b0 = task.a0; sw.nb = task.na;
+        sw.pa0 = task.pb0; sw.pb0 = task.pa0; sw.nprim_a = task.nprim_b; sw.nprim_b = task.nprim_a;
+        sw.rows_are_b = !task.rows_are_b;
+        // an s-s ket pair against a large bra pair ((fd|ss), (ff|ss)): split
+        // the bra's first shell instead, with bra and ket exchanged
+        constexpr int CKS = SMALL_NF / (N34 * ncart(L2));
+        constexpr int NCHS = (NCH == 0 && N34 == 1 && CKS >= 1) ? cdiv(ncart(L1), CKS) : 0;
+        if constexpr (NCHS >= 1 && NCHS <= MAX_SPLIT) {
+            const int v = bqc_class_variant(L1, L2, L3, L4);
+            if (v == BQC_VARIANT_SPLIT || v == BQC_VARIANT_AUTO)
+                return launch_split<L3, L4, L1, L2, CKS>(jk_args_swap_eri(args), sw, fp32, stream);
+        }
         if constexpr (N12 <= N34) {
             constexpr int NS = cdiv(N34, 36) > ncart(L3) ? ncart(L3) : cdiv(N34, 36);
             return launch_group<L1, L2, L3, L4, NS>(args, task, fp32, stream);
         } else {
             constexpr int NS = cdiv(N12, 36) > ncart(L1) ? ncart(L1) : cdiv(N12, 36);
-            JKTask sw = task;
-            sw.a0 = task.b0; sw.na = task.nb; sw.b0 = task.a0; sw.nb = task.na;
-            sw.pa0 = task.pb0; sw.pb0 = task.pa0; sw.nprim_a = task.nprim_b; sw.nprim_b = task.nprim_a;
-            sw.rows_are_b = !task.rows_are_b;
-            // diag tasks have identical lists on both sides; the a >= b rule stays
             return launch_group<L3, L4, L1, L2, NS>(jk_args_swap_eri(args), sw, fp32, stream);
         }
     }

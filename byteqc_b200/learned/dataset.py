@@ -39,13 +39,14 @@ def pair_frames(mol):
     return PairFrames(mol)
 
 
-def samples(mol, dm, dm_sad):
+def samples(mol, dm, dm_sad, out_dim=OUT_DIM, dtype=np.float64):
     """Features, targets (local-frame block minus local SAD block, padded to
-    OUT_DIM) and masks of every canonical pair of mol."""
+    out_dim) and masks of every canonical pair of mol; the training set
+    keeps them in FP32 (dtype), which is what the network trains on."""
     pf = PairFrames(mol)
     P = len(pf.pairs)
-    tgt = np.zeros((P, OUT_DIM))
-    mask = np.zeros((P, OUT_DIM))
+    tgt = np.zeros((P, out_dim), dtype=dtype)
+    mask = np.zeros((P, out_dim), dtype=dtype)
     diff = dm - dm_sad
     for idx, a, b, Ua, Ub in pf.groups:
         na, nb = Ua.shape[1], Ub.shape[1]

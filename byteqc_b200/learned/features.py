@@ -27,6 +27,8 @@ ANG = 0.52917721092           # Angstrom per Bohr
 PAIR_CUTOFF = 5.0             # Angstrom
 FEAT_DIM = 64
 OUT_DIM = 208                 # >= 14 x 14 (largest DZ-shaped block), multiple of 16
+# output width per basis shape: the largest atom-pair block, rounded up to 16
+OUT_DIMS = {'cc-pvdz': 208, 'cc-pvtz': 912}   # 14 x 14 and 30 x 30 AOs
 ELEMENT_RANK = {'O': 3, 'N': 2, 'C': 1, 'H': 0}
 PAIR_TYPES = ['O', 'C', 'H', 'OO', 'CC', 'HH', 'OH', 'CH', 'OC']
 RBF_CENTRES = np.linspace(0.5, 6.0, 16)

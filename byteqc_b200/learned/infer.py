@@ -9,7 +9,16 @@ from .model import DensityMLP
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_WEIGHTS = os.path.join(HERE, 'weights_ccpvdz.npz')
+# trained models per basis shape
+WEIGHTS = {'cc-pvdz': DEFAULT_WEIGHTS, 'cc-pvtz': os.path.join(HERE, 'weights_ccpvtz.npz')}
 _MODELS = {}
+
+
+def weights_for(mol):
+    """The trained weights for the basis shape of mol (mol.basis_name, the
+    cc-pVDZ shape when it is not set), or None when none was trained."""
+    path = WEIGHTS.get(getattr(mol, 'basis_name', 'cc-pvdz'))
+    return path if path is not None and os.path.exists(path) else None
 
 
 def load_model(path=DEFAULT_WEIGHTS):

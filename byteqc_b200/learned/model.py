@@ -13,7 +13,13 @@ from .. import lib as _libmod
 from .features import FEAT_DIM, OUT_DIM
 
 WIDTH = 256
-LAYERS = [(WIDTH, FEAT_DIM), (WIDTH, WIDTH), (WIDTH, WIDTH), (OUT_DIM, WIDTH)]
+
+
+def layers(out_dim=OUT_DIM):
+    return [(WIDTH, FEAT_DIM), (WIDTH, WIDTH), (WIDTH, WIDTH), (out_dim, WIDTH)]
+
+
+LAYERS = layers()
 
 
 def _vp(t):
@@ -25,12 +31,13 @@ def _stream():
 
 
 class DensityMLP:
-    def __init__(self, seed=0, device='cuda'):
+    def __init__(self, seed=0, device='cuda', out_dim=OUT_DIM):
         self.lib = _libmod.load_library()
         self.device = torch.device(device)
+        self.layers = layers(out_dim)
         rng = np.random.default_rng(seed)
         self.W, self.b = [], []
-        for n, k in LAYERS:
+        for n, k in self.layers:
             w = rng.normal(size=(n, k)) * np.sqrt(2. / k)
             self.W.append(torch.as_tensor(w, dtype=torch.float32, device=self.device))
             self.b.append(torch.zeros(n, dtype=torch.float32, device=self.device))
@@ -48,7 +55,8 @@ class DensityMLP:
                {'b%d' % i: b.cpu().numpy() for i, b in enumerate(self.b)}
 
     def load(self, state):
-        for i in range(len(LAYERS)):
+        self.layers = layers(int(state['W%d' % (len(self.layers) - 1)].shape[0]))
+        for i in range(len(self.layers)):
             self.W[i] = torch.as_tensor(state['W%d' % i], dtype=torch.float32, device=self.device)
             self.b[i] = torch.as_tensor(state['b%d' % i], dtype=torch.float32, device=self.device)
         self._sync_bf16()
@@ -61,8 +69,8 @@ class DensityMLP:
         M = x.shape[0]
         h = x.to(torch.bfloat16).contiguous()
         acts, zs = [h], []
-        for i, (n, k) in enumerate(LAYERS):
-            last = i == len(LAYERS) - 1
+        for i, (n, k) in enumerate(self.layers):
+            last = i == len(self.layers) - 1
             z = torch.empty((M, n), dtype=torch.float32, device=self.device)
             yb = None if last else torch.empty((M, n), dtype=torch.bfloat16, device=self.device)
             err = self.lib.BQCmlp_linear_fwd(_vp(h), _vp(self.Wb[i]), _vp(self.b[i]), _vp(z), None,
@@ -83,11 +91,11 @@ class DensityMLP:
         Returns FP32 gradients [dW...] + [db...]."""
         acts, zs = self._cache
         M = dy.shape[0]
-        dWs, dbs = [None] * len(LAYERS), [None] * len(LAYERS)
+        dWs, dbs = [None] * len(self.layers), [None] * len(self.layers)
         g = dy.contiguous()
-        for i in reversed(range(len(LAYERS))):
-            n, k = LAYERS[i]
-            last = i == len(LAYERS) - 1
+        for i in reversed(range(len(self.layers))):
+            n, k = self.layers[i]
+            last = i == len(self.layers) - 1
             dW = torch.empty((n, k), dtype=torch.float32, device=self.device)
             db = torch.empty(n, dtype=torch.float32, device=self.device)
             dx = torch.empty((M, k), dtype=torch.float32, device=self.device) if i > 0 else None

@@ -41,9 +41,11 @@ def training_systems(nsys, seed=0):
     return out
 
 
-def make_mol(atoms):
+def make_mol(atoms, basis=None):
     els = sorted(set(a[0] for a in atoms))
-    return Mole(atoms, synthetic_basis(BASIS, els))
+    mol = Mole(atoms, synthetic_basis(basis or BASIS, els))
+    mol.basis_name = (basis or BASIS).lower()
+    return mol
 
 
 def converged(mol, conv=1e-9):
@@ -54,16 +56,18 @@ def converged(mol, conv=1e-9):
     return mf, mf.dm.cpu().numpy(), sad.cpu().numpy()
 
 
-def collect(systems, log=print):
+def collect(systems, log=print, basis=None):
+    from .features import OUT_DIMS
+    out_dim = OUT_DIMS[(basis or BASIS).lower()]
     F, T, K = [], [], []
     t0 = time.time()
     cache = {}
     for i, (kind, size, seed, atoms) in enumerate(systems):
         key = (kind, size, seed)
         if key not in cache:
-            mol = make_mol(atoms)
+            mol = make_mol(atoms, basis)
             mf, dm, sad = converged(mol)
-            cache[key] = dataset.samples(mol, dm, sad)
+            cache[key] = dataset.samples(mol, dm, sad, out_dim, np.float32)
         f, t, k = cache[key]
         F.append(f)
         T.append(t)
@@ -75,7 +79,7 @@ def collect(systems, log=print):
 
 def fit(F, T, K, epochs=200, batch=4096, lr=1e-3, seed=0, log=print):
     dev = torch.device('cuda')
-    model = DensityMLP(seed=seed)
+    model = DensityMLP(seed=seed, out_dim=T.shape[1])
     Fd = torch.as_tensor(F, dtype=torch.float32, device=dev)
     Td = torch.as_tensor(T, dtype=torch.float32, device=dev)
     Kd = torch.as_tensor(K, dtype=torch.float32, device=dev)
@@ -104,12 +108,12 @@ def fit(F, T, K, epochs=200, batch=4096, lr=1e-3, seed=0, log=print):
     return model, hist
 
 
-def evaluate(model_path, log=print):
+def evaluate(model_path, log=print, basis=None):
     """SCF cycles and time from SAD and from the learned guess on held-out
     (H2O)_32 (seed 7) and C40H82."""
     out = {}
     for name, atoms in (('(H2O)32', water_cluster(32, seed=7)), ('C40H82', linear_alkane(40))):
-        mol = make_mol(atoms)
+        mol = make_mol(atoms, basis)
         rec = {}
         for guess in ('sad', 'mlp'):
             from ..learned import infer
@@ -117,6 +121,7 @@ def evaluate(model_path, log=print):
             mf = hf.RHF(mol)
             mf.conv_tol = 1e-9
             mf.init_guess = guess
+            mf.mlp_weights = model_path
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             e = mf.kernel()
@@ -136,18 +141,19 @@ def main(argv=None):
     ap.add_argument('--epochs', type=int, default=200)
     ap.add_argument('--out', default=None)
     ap.add_argument('--report', default=None)
+    ap.add_argument('--basis', default=BASIS)
     a = ap.parse_args(argv)
     t0 = time.time()
-    F, T, K = collect(training_systems(a.nsys))
+    F, T, K = collect(training_systems(a.nsys), basis=a.basis)
     t_data = time.time() - t0
     print('samples', F.shape, 'data %.0f s' % t_data, flush=True)
     t0 = time.time()
     model, hist = fit(F, T, K, epochs=a.epochs)
     t_fit = time.time() - t0
     out = a.out or __import__('os').path.join(__import__('os').path.dirname(__file__),
-                                              'weights_ccpvdz.npz')
+                                              'weights_%s.npz' % a.basis.replace('-', ''))
     np.savez(out, **model.state())
-    ev = evaluate(out)
+    ev = evaluate(out, basis=a.basis)
     rep = {'nsys': a.nsys, 'samples': int(F.shape[0]), 'epochs': a.epochs,
            'data_seconds': t_data, 'fit_seconds': t_fit, 'loss_first': hist[0],
            'loss_last': hist[-1], 'eval': ev}

@@ -74,8 +74,12 @@ def init_guess(mf, kind='sad'):
         c = c[:, torch.argsort(e)[:nocc]]
         return 2. * c @ c.T
     if kind == 'mlp':
-        from ..learned.infer import mlp_density, DEFAULT_WEIGHTS
-        return mlp_density(mf, init_guess(mf, 'sad'), getattr(mf, 'mlp_weights', DEFAULT_WEIGHTS))
+        from ..learned.infer import mlp_density, weights_for
+        path = getattr(mf, 'mlp_weights', None) or weights_for(mol)
+        if path is None:
+            raise FileNotFoundError('no trained density model for the basis shape %r'
+                                    % getattr(mol, 'basis_name', 'cc-pvdz'))
+        return mlp_density(mf, init_guess(mf, 'sad'), path)
     if kind not in ('sad', 'minao', 'atom'):
         raise ValueError('unknown init_guess %r' % kind)
     nao = mol.nao

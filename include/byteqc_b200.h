@@ -229,8 +229,10 @@ int BQCmlp_to_bf16(const float *x, void *y, size_t n, cudaStream_t stream);
 /* Kernel choice for shell-quartet class (li lj | lk ll) in this process, any
  * order of the four: variant 0 = built-in rule, 1 = group kernel (threads
  * per quartet share the 2D tables in shared memory), 2 = ket-split tile
- * kernel (one thread per quartet, shell k's components in a few launches;
- * only classes that split into at most 3 such launches, others ignore it).
+ * kernel (one thread per quartet, shell k's components in a few launches,
+ * or for an s-s ket against a large bra pair the bra's first shell with bra
+ * and ket exchanged; only classes that split into at most 3 such launches,
+ * others ignore it).
  * The choice changes speed only, never results.  Returns 0, 2 for l > 3,
  * 3 for an unknown variant.  No reference counterpart (the reference has one
  * fixed kernel per class, cuobc/lib/gvhf/nr_jk_driver.cu:40-225). */

@@ -165,7 +165,8 @@ def test_autotune_variant_rule():
                    [(a, b, c, d) for a in range(4) for b in range(4) for c in range(4) for d in range(4)]
                    if autotune.has_variants(*c)})
     assert both == [(1, 1, 1, 1), (2, 1, 1, 1), (2, 1, 2, 0), (2, 2, 1, 0),
-                    (3, 0, 1, 1), (3, 0, 2, 0), (3, 0, 3, 0), (3, 1, 1, 0)]
+                    (3, 0, 1, 1), (3, 0, 2, 0), (3, 0, 3, 0), (3, 1, 1, 0), (3, 2, 0, 0),
+                    (3, 3, 0, 0)]
     assert autotune.canonical(0, 1, 2, 2) == (2, 2, 1, 0)
 
 
