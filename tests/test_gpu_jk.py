@@ -357,3 +357,20 @@ def test_device_schedule_matches_host_pruning(cuda, fp32_below):
     assert float((j1 - j0).abs().max()) < 1e-12 * max(1., float(j0.abs().max()))
     assert float((k1 - k0).abs().max()) < 1e-12 * max(1., float(k0.abs().max()))
     assert float(j0.abs().max()) > 0
+
+
+def test_repeated_builds_agree(cuda):
+    """Two builds of the same density differ only by the order of the FP64
+    atomic additions: at most a few units in the last place of the largest
+    element (bound 1e-13 relative)."""
+    import torch
+    from byteqc_b200.scf import hf
+    mol = _mol('cc-pvtz', nw=3, seed=13)
+    opt = hf._VHFOpt(mol).build()
+    dm = torch.as_tensor(_rand_dm(mol.nao, 17) * 0.1, device=cuda)[None]
+    vj0, vk0 = opt.jk_ao(dm)
+    vj1, vk1 = opt.jk_ao(dm)
+    dj = float((vj1 - vj0).abs().max()) / float(vj0.abs().max())
+    dk = float((vk1 - vk0).abs().max()) / float(vk0.abs().max())
+    print('repeat: relative max|dJ| %.2e max|dK| %.2e' % (dj, dk))
+    assert dj < 1e-13 and dk < 1e-13
