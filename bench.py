@@ -276,8 +276,10 @@ def cpu_oracle_scf(threads):
 
 
 # DRAM bytes per launch of the J/K kernels (dram__bytes_read.sum +
-# dram__bytes_write.sum of one ncu capture), by class; see profiles/.
-TRAFFIC = {}
+# dram__bytes_write.sum of one ncu --set full capture of one launch of the
+# class at (H2O)_64 / cc-pVTZ shape on the jk.py density), by class
+TRAFFIC = {'(ps|ss)': 72824320 + 38084352, '(dp|ps)': 300668672 + 132837376,
+           '(fp|dp)': 570294016 + 3547033000}
 
 
 def main():

@@ -77,3 +77,33 @@ def assemble(mol, pf, pred, dm_sad):
             np.add.at(dm, (c[off].transpose(0, 2, 1), r[off].transpose(0, 2, 1)),
                       blk[off].transpose(0, 2, 1))
     return dm
+
+
+def assemble_device(mol, pf, pred, dm_sad):
+    """assemble() on the device: pred (pairs x width) and dm_sad are torch
+    tensors; the blocks are rotated back with batched matrix products and
+    added with one index_add per element pair."""
+    import torch
+    dev = dm_sad.device
+    nao = dm_sad.shape[-1]
+    dm = dm_sad.clone()
+    flat = dm.view(-1)
+    for idx, a, b, Ua, Ub in pf.groups:
+        na, nb = Ua.shape[1], Ub.shape[1]
+        it = torch.as_tensor(idx, device=dev)
+        loc = pred[it, :na * nb].to(torch.float64).reshape(len(idx), na, nb)
+        Ua_t = torch.as_tensor(Ua, dtype=torch.float64, device=dev)
+        Ub_t = torch.as_tensor(Ub, dtype=torch.float64, device=dev)
+        blk = Ua_t.transpose(1, 2) @ loc @ Ub_t                  # U_a^T loc U_b
+        r, c = pf._index(a, b, na, nb)
+        lin = torch.as_tensor((r * nao + c).astype(np.int64), device=dev)       # (G, na, nb)
+        lin_t = torch.as_tensor((c * nao + r).astype(np.int64), device=dev)
+        on = torch.as_tensor(a == b, device=dev)
+        if bool((a == b).any()):
+            sym = 0.5 * (blk[on] + blk[on].transpose(1, 2))
+            flat.index_add_(0, lin[on].reshape(-1), sym.reshape(-1))
+        off = ~on
+        if bool((a != b).any()):
+            flat.index_add_(0, lin[off].reshape(-1), blk[off].reshape(-1))
+            flat.index_add_(0, lin_t[off].reshape(-1), blk[off].reshape(-1))
+    return dm

@@ -37,9 +37,8 @@ def mlp_density(mf, dm_sad=None, path=DEFAULT_WEIGHTS):
         dm_sad = init_guess(mf, 'sad')
     model = load_model(path)
     pf = dataset.pair_frames(mol)
-    pred = model.predict(pf.feats).cpu().numpy().astype(np.float64)
-    dm = dataset.assemble(mol, pf, pred, dm_sad.cpu().numpy())
-    dm = torch.as_tensor(dm, device=dm_sad.device)
+    pred = model.predict(pf.feats)
+    dm = dataset.assemble_device(mol, pf, pred, dm_sad)
     ne = float(torch.sum(dm * mf.get_ovlp()))
     if ne > 0:
         dm *= mol.nelectron / ne

@@ -1,10 +1,7 @@
 """Parity of the device J/K engine with the CPU oracle (needs a B200).
 
 Tolerances: J and K max-abs error <= 1e-10 in plain FP64 (the bar of the
-drop-in), SCF total energy within 1e-9 Eh.  Where a test's density makes |J|
-reach several hundred, the 1e-10 bar applies to J/max(1, |J|max/100): both
-sides sum O(10^5) FP64 terms per element, whose rounding alone reaches a few
-1e-15 relative; every such case states it.
+drop-in), SCF total energy within 1e-9 Eh.
 """
 import numpy as np
 import pytest
@@ -40,9 +37,7 @@ def test_jk_water(cuda, kind):
     rj, rk = oracle.get_jk(mol, dm)
     ej, ek = abs(vj - rj).max(), abs(vk - rk).max()
     print('water %s: max|J| %.3g max|dJ| %.3e max|dK| %.3e' % (kind, abs(rj).max(), ej, ek))
-    # |J| reaches ~400 with this density: relative bar (module doc)
-    assert ej < TOL_JK * max(1, abs(rj).max() / 100)
-    assert ek < TOL_JK * max(1, abs(rk).max() / 100)
+    assert ej < TOL_JK and ek < TOL_JK
 
 
 @pytest.mark.parametrize('variant', [1, 2])
@@ -101,9 +96,7 @@ def test_jk_two_waters_tz(cuda):
     rj, rk = oracle.get_jk(mol, dm)
     ej, ek = abs(vj - rj).max(), abs(vk - rk).max()
     print('TZ dimer: max|J| %.3g max|dJ| %.3e max|dK| %.3e' % (abs(rj).max(), ej, ek))
-    # |J| reaches ~1e3 with this density: relative bar (module doc)
-    assert ej < TOL_JK * max(1, abs(rj).max() / 100)
-    assert ek < TOL_JK * max(1, abs(rk).max() / 100)
+    assert ej < TOL_JK and ek < TOL_JK
 
 
 def test_schwarz_and_int1e(cuda):
@@ -166,9 +159,8 @@ def test_gint_abi_matches_native(cuda):
     rj, rk = oracle.get_jk(mol, dm)
     print('GINT ABI: max|J| %.3g max|dJ| %.3e max|dK| %.3e' % (abs(rj).max(), abs(J - rj).max(),
                                                              abs(K - rk).max()))
-    # |J| reaches ~500 with this density: relative bar (module doc)
-    assert abs(J - rj).max() < TOL_JK * max(1, abs(rj).max() / 100)
-    assert abs(K - rk).max() < TOL_JK * max(1, abs(rk).max() / 100)
+    assert abs(J - rj).max() < TOL_JK
+    assert abs(K - rk).max() < TOL_JK
 
 
 def test_rhf_energy(cuda):

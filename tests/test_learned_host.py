@@ -59,3 +59,19 @@ def test_assemble_inverts_samples():
     f, t, k = dataset.samples(mol, d, sad)
     back = dataset.assemble(mol, dataset.pair_frames(mol), t, sad)
     assert np.abs(back - d).max() < 1e-10
+
+
+def test_device_assembly_matches_host():
+    """assemble_device (torch, here on the CPU) adds the same blocks as the
+    numpy assembly, for both basis shapes."""
+    import torch
+    for kind, width in (('cc-pvdz', 208), ('cc-pvtz', 912)):
+        mol = Mole(water_cluster(3, seed=2), synthetic_basis(kind, ['O', 'H']))
+        pf = dataset.pair_frames(mol)
+        rng = np.random.default_rng(1)
+        pred = rng.normal(size=(len(pf.pairs), width))
+        sad = rng.normal(size=(mol.nao, mol.nao))
+        ref = dataset.assemble(mol, pf, pred, sad)
+        got = dataset.assemble_device(mol, pf, torch.as_tensor(pred), torch.as_tensor(sad)).numpy()
+        assert np.abs(got - ref).max() < 1e-12
+        assert np.abs(got - got.T).max() < 1e-12 + np.abs(sad - sad.T).max()
