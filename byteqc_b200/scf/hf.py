@@ -541,14 +541,23 @@ def _jk_schwarz_only(vhfopt, dmc, with_j, with_k):
     return vj, vk
 
 
-def eig(h, s):
-    """Generalized eigenproblem h C = s C e by canonical orthogonalisation
-    (cuobc/scf/hf.py:253-265), on the device."""
-    h = torch.as_tensor(h, device=_dev())
+def orthogonalizer(s):
+    """The canonical orthogonalisation of the overlap s: its eigenvectors
+    scaled by 1/sqrt(eigenvalue), zero columns for eigenvalues below 1e-15
+    (cuobc/scf/hf.py:253-265)."""
     s = torch.as_tensor(s, device=_dev())
     seig, t = torch.linalg.eigh(s)
     inv = torch.where(seig < 1e-15, torch.zeros_like(seig), 1. / torch.sqrt(seig))
-    t = t * inv
+    return t * inv
+
+
+def eig(h, s, t=None):
+    """Generalized eigenproblem h C = s C e by canonical orthogonalisation
+    (cuobc/scf/hf.py:253-265), on the device; t: the orthogonalizer of s
+    when the caller already has it."""
+    h = torch.as_tensor(h, device=_dev())
+    if t is None:
+        t = orthogonalizer(s)
     e, c = torch.linalg.eigh(t.T @ h @ t)
     return e, t @ c
 
@@ -585,7 +594,13 @@ class _SCFBase:
         return get_jk(mol or self.mol, dm, hermi, self.opt, with_j, with_k)
 
     def _eigh(self, h, s):
-        return eig(h, s)
+        # the overlap does not change during an SCF: its orthogonalizer is
+        # computed once per overlap object (the reference recomputes it in
+        # every call of eig)
+        cached = getattr(self, '_orth', None)
+        if cached is None or cached[0] is not s:
+            cached = self._orth = (s, orthogonalizer(s))
+        return eig(h, s, cached[1])
 
     def get_ovlp(self):
         return self._ints()[0]
