@@ -72,7 +72,19 @@ struct JKTask {
     // grid holds at most a few CTAs per SM of the nsm SMs.
     const int *ntiles_dev;
     int nsm;
+    // parts per tile of a group-kernel launch without ntiles_dev (set by the
+    // launcher; with ntiles_dev the kernel derives it from the device count)
+    int split;
 };
+
+// Parts a group-kernel tile is cut into: a launch with fewer than 16 tiles
+// per SM cuts each tile into 2, 4 or 8 interleaved parts (one CTA each), so
+// that small builds still fill every SM; larger ones keep one CTA per tile.
+__host__ __device__ inline int group_split(int ntiles, int nsm) {
+    int s = 1;
+    while (s < 8 && (long long)ntiles * s < 16LL * nsm) s *= 2;
+    return s;
+}
 
 // grid of a launch over ntiles tiles of per_tile CTAs each; persistent
 // launches cap it at ctas_per_sm CTAs on each SM

@@ -92,9 +92,14 @@ __device__ __forceinline__ void tile_of_block(const JKTask &T, int x, int &r, in
     }
 }
 
+// Surviving quartets of tile x into s_list (order unspecified).  With
+// nparts > 1 (a power of two up to 16) only the quartets e = part (mod
+// nparts) of the tile's 256 are screened, e = 16 * row + column: part p takes
+// every nparts-th column of every row, so the parts are disjoint, cover the
+// tile and get similar shares of a q-sorted tile.
 __device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, int x, int *s_list,
                                             int *s_count, int &a_begin, int &b_begin,
-                                            int &count) {
+                                            int &count, int part = 0, int nparts = 1) {
     int r, c;
     tile_of_block(T, x, r, c);
     int ta = T.rows_are_b ? c : r, tb = T.rows_are_b ? r : c;
@@ -105,7 +110,8 @@ __device__ __forceinline__ bool tile_screen(const JKArgs &A, const JKTask &T, in
     if (T.diag && b_begin > a_end - 1) return false;
     if (threadIdx.x == 0) *s_count = 0;
     __syncthreads();
-    for (int e = threadIdx.x; e < TILE * TILE; e += blockDim.x) {
+    for (int e0 = threadIdx.x; e0 < TILE * TILE / nparts; e0 += blockDim.x) {
+        const int e = e0 * nparts + part;
         int a = a_begin + e / TILE, b = b_begin + e % TILE;
         bool keep = a < a_end && b < b_end && (!T.diag || a >= b);
         if (keep && A.pair_q != nullptr) {
@@ -626,9 +632,9 @@ jk_group(JKArgs A, JKTask T) {
     extern __shared__ double smem[];
     __shared__ int s_list[TILE * TILE];
     __shared__ int s_count;
-    auto tile = [&](const int x) {
+    auto tile = [&](const int x, const int part, const int nparts) {
     int a_begin, b_begin, count;
-    if (!tile_screen(A, T, x, s_list, &s_count, a_begin, b_begin, count)) return;
+    if (!tile_screen(A, T, x, s_list, &s_count, a_begin, b_begin, count, part, nparts)) return;
 
     const int g = threadIdx.x / TPQ;
     const int lane = threadIdx.x % TPQ;
@@ -902,9 +908,18 @@ jk_group(JKArgs A, JKTask T) {
         }
     }
     };
-    const int ntiles = T.ntiles_dev == nullptr ? (int)gridDim.x : __ldg(T.ntiles_dev);
-    for (int x = blockIdx.x; x < ntiles; x += gridDim.x) {
-        tile(x);
+    // virtual block vb = part vb % S of tile vb / S
+    int S, nvb;
+    if (T.ntiles_dev == nullptr) {
+        S = T.split;
+        nvb = (int)gridDim.x;
+    } else {
+        const int n = __ldg(T.ntiles_dev);
+        S = group_split(n, T.nsm);
+        nvb = n * S;
+    }
+    for (int vb = blockIdx.x; vb < nvb; vb += gridDim.x) {
+        tile(vb / S, vb % S, S);
         __syncthreads();
     }
 }
@@ -931,6 +946,19 @@ static int smem_attr(int bytes) {
         done[dev].store(1, std::memory_order_release);
     }
     return 0;
+}
+
+// SM count of the current device (cached per device; 0 on error)
+static inline int device_sms() {
+    static std::atomic<int> sms[MAX_DEVICES];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= MAX_DEVICES) return 0;
+    int n = sms[dev].load(std::memory_order_relaxed);
+    if (n == 0) {
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+        sms[dev].store(n, std::memory_order_relaxed);
+    }
+    return n;
 }
 
 template <int LI, int LJ, int LK, int LL, typename F, int K0, int KN>
@@ -976,7 +1004,17 @@ static int launch_group_f(const JKArgs &args, const JKTask &task, cudaStream_t s
     int ntiles = task.tile_prefix ? task.ntiles : task_tiles(task);
     if (ntiles == 0) return 0;
     if (smem_attr<jk_group<LI, LJ, LK, LL, NSPLIT, F>>((int)C::SMEM)) return 1;
-    jk_group<LI, LJ, LK, LL, NSPLIT, F><<<bqc_grid(task, ntiles, 1, 8), C::NT, C::SMEM, stream>>>(args, task);
+    JKTask t = task;
+    int grid;
+    if (t.ntiles_dev == nullptr) {
+        const int nsm = t.nsm > 0 ? t.nsm : device_sms();
+        if (nsm <= 0) return 1;
+        t.split = group_split(ntiles, nsm);
+        grid = ntiles * t.split;
+    } else {
+        grid = bqc_grid(t, ntiles, 8, 8);   // the kernel cuts tiles into at most 8 parts
+    }
+    jk_group<LI, LJ, LK, LL, NSPLIT, F><<<grid, C::NT, C::SMEM, stream>>>(args, t);
     return 0;
 }
 
