@@ -644,6 +644,48 @@ class _SCFBase:
         return torch.einsum('i,i...->...', c, torch.stack(self._diis_f))
 
 
+class HostDIIS:
+    """Pulay DIIS on host numpy arrays, the role pyscf's lib.diis.DIIS plays
+    in the reference's CPU SCF loop: the Gram matrix of the error vectors is
+    kept and extended by one row per cycle (n dot products instead of an
+    n x n product over copies of every stored vector), and the extrapolated
+    Fock matrix is accumulated in place."""
+
+    def __init__(self, space=8):
+        self.space = space
+        self.focks, self.errs = [], []
+        self.gram = np.zeros((0, 0))
+
+    def update(self, F, err):
+        """Store (F, err) and return the extrapolated Fock matrix."""
+        err = np.ascontiguousarray(err).ravel()
+        if len(self.focks) == self.space:
+            self.focks.pop(0)
+            self.errs.pop(0)
+            self.gram = self.gram[1:, 1:]
+        row = np.array([float(np.dot(e, err)) for e in self.errs] + [float(np.dot(err, err))])
+        n = len(row)
+        g = np.empty((n, n))
+        g[:n - 1, :n - 1] = self.gram
+        g[n - 1, :] = row
+        g[:, n - 1] = row
+        self.gram = g
+        self.focks.append(F)
+        self.errs.append(err)
+        if n < 2:
+            return F
+        B = -np.ones((n + 1, n + 1))
+        B[n, n] = 0
+        B[:n, :n] = g
+        rhs = np.zeros(n + 1)
+        rhs[n] = -1
+        c = np.linalg.solve(B, rhs)[:n]
+        Fd = self.focks[0] * c[0]
+        for ci, Fi in zip(c[1:], self.focks[1:]):
+            Fd += ci * Fi
+        return Fd
+
+
 class RHF(_SCFBase):
     """Restricted Hartree-Fock; the J/K builds go through the device engine.
 
@@ -796,7 +838,7 @@ class RHF(_SCFBase):
         nao = dm.shape[0]
         nocc = self.mol.nelectron // 2
         h2d = d2h = 0
-        focks, errs = [], []
+        diis = HostDIIS(self.diis_space)
         e_last = None
         vj = vk = dm_last = None
         self.converged = False
@@ -828,21 +870,10 @@ class RHF(_SCFBase):
             if mixed and not final and de < self.mixed_switch_tol:
                 final = True
             e_last = e
-            focks.append(F)
-            errs.append((F @ dm @ S - S @ dm @ F).ravel())
-            focks, errs = focks[-self.diis_space:], errs[-self.diis_space:]
-            n = len(focks)
-            if n > 1:
-                B = -np.ones((n + 1, n + 1))
-                B[n, n] = 0
-                E = np.array(errs)
-                B[:n, :n] = E @ E.T
-                rhs = np.zeros(n + 1)
-                rhs[n] = -1
-                c = np.linalg.solve(B, rhs)[:n]
-                Fd = np.einsum('i,ijk->jk', c, np.array(focks))
-            else:
-                Fd = F
+            # F D S - S D F = X - X^T with X = F D S (F, D, S symmetric), as
+            # pyscf forms the DIIS error
+            X = F @ dm @ S
+            Fd = diis.update(F, X - X.T)
             mo_e, mo_c = self._eigh(Fd, S)
             mo_e = mo_e.cpu().numpy()
             mo_c = mo_c.cpu().numpy()

@@ -174,6 +174,26 @@ def test_rhf_energy(cuda):
     assert abs(e - e_ref) < 1e-9
 
 
+def test_host_loop_matches_device_loop(cuda):
+    """The drop-in arrangement (host numpy SCF loop, get_jk with host
+    densities, host DIIS) converges to the device loop's energy, in plain
+    FP64 and in the fast form."""
+    from byteqc_b200.scf import hf
+    mol = _mol('cc-pvdz', nw=2, seed=1)
+    for fast in (False, True):
+        ms = []
+        for host in (False, True):
+            mf = hf.RHF(mol)
+            mf.conv_tol = 1e-10
+            if fast:
+                mf.fp32_threshold = 1e-4
+                mf.early_tol = 1e-10
+            e = mf.kernel_hostloop() if host else mf.kernel()
+            assert mf.converged
+            ms.append(e)
+        assert abs(ms[0] - ms[1]) < 1e-9, (fast, ms)
+
+
 def test_uhf_closed_shell_equals_rhf(cuda):
     from byteqc_b200.scf import hf
     mol = _mol('cc-pvdz', nw=1, seed=2)

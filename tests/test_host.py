@@ -278,3 +278,35 @@ def opt_i_ge(i, j, offs):
     gi = np.searchsorted(offs, i, side='right')
     gj = np.searchsorted(offs, j, side='right')
     return gi > gj or (gi == gj and i >= j)
+
+
+def test_host_diis_matches_full_solve():
+    """HostDIIS (incremental Gram matrix, in-place extrapolation) gives the
+    Fock matrix of a full Pulay solve over the last `space` stored pairs."""
+    from byteqc_b200.scf.hf import HostDIIS
+    rng = np.random.default_rng(5)
+    n, space = 12, 4
+    diis = HostDIIS(space)
+    focks, errs = [], []
+    for it in range(9):
+        F = rng.normal(size=(n, n))
+        F = F + F.T
+        X = F @ rng.normal(size=(n, n))
+        err = X - X.T
+        got = diis.update(F, err)
+        focks.append(F)
+        errs.append(err.ravel())
+        fs, es = focks[-space:], np.array(errs[-space:])
+        m = len(fs)
+        if m < 2:
+            assert got is F
+            continue
+        B = -np.ones((m + 1, m + 1))
+        B[m, m] = 0
+        B[:m, :m] = es @ es.T
+        rhs = np.zeros(m + 1)
+        rhs[m] = -1
+        c = np.linalg.solve(B, rhs)[:m]
+        ref = np.einsum('i,ijk->jk', c, np.array(fs))
+        assert np.abs(got - ref).max() < 1e-10 * max(1., np.abs(ref).max())
+        assert np.abs(diis.gram - es @ es.T).max() < 1e-10 * np.abs(es @ es.T).max()
