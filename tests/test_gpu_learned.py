@@ -4,7 +4,7 @@ B200 and the trained weights in byteqc_b200/learned/).
 On held-out systems (the training set is seeded (H2O)_k with k in [2, 16]
 and CnH(2n+2) with n in [4, 20]): the plain FP64 RHF from the learned guess
 and from SAD converge to the same energy (within 1e-9 Eh: the converged FP64
-SCF is the judge, only the iteration count may change), and the learned
+SCF fixes the energy, only the iteration count may change), and the learned
 guess needs fewer SCF cycles in total.  Cycles and wall times are printed.
 """
 import time
