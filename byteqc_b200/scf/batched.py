@@ -7,7 +7,10 @@ grouped by molecule and sorted by their largest Schwarz factor), so one
 class pair; quartets never mix molecules.  The AO densities and J/K live in
 one block-diagonal matrix over all molecules (HBM holds it easily: 51k
 Cartesian AOs for 256 (H2O)_k, k <= 12); the SCF linear algebra (DIIS,
-generalized eigenproblem, density, energy) runs batched over a padded stack.
+density, energy) runs batched over a padded stack, and the new density of
+each cycle is the occupied projector of the orthogonalised Fock matrix by
+canonical purification, batched GEMMs per molecule size (an eigensolver only
+for a molecule without a gap at the Fermi level).
 """
 import ctypes
 import time
@@ -20,6 +23,104 @@ from ..gto import mole as gto
 from .hf import (_VHFOpt, _dev, _ptr, _stream, basis_seg_contraction, _tile_order, PAIR_TILE,
                  free_basis_cache, make_plan)
 from .guess import atomic_density
+
+
+def _intra_pairs(sp, sq, shell_mol, nmol, diag):
+    """Shell pairs (i in sp, j in sq) of the same molecule, i-major then j
+    ascending (i >= j when diag).  sp and sq are ascending and the shells of a
+    molecule are contiguous, so each molecule's members of sp (and of sq) form
+    one run: the pairs are generated molecule by molecule by index arithmetic,
+    in time proportional to their number rather than to len(sp) * len(sq)."""
+    cp = np.bincount(shell_mol[sp], minlength=nmol)
+    cq = np.bincount(shell_mol[sq], minlength=nmol)
+    p0 = np.r_[0, np.cumsum(cp)[:-1]]
+    q0 = np.r_[0, np.cumsum(cq)[:-1]]
+    npair = cp * cq
+    m = np.repeat(np.arange(nmol), npair)
+    t = np.arange(int(npair.sum())) - np.r_[0, np.cumsum(npair)[:-1]][m]
+    i = sp[p0[m] + t // cq[m]]
+    j = sq[q0[m] + t % cq[m]]
+    if diag:
+        keep = i >= j
+        i, j = i[keep], j[keep]
+    return i, j
+
+
+def _eigh_by_size(A, sizes):
+    """Eigenpairs of the padded stack A (B, n, n) solved molecule size by
+    molecule size on the leading sizes[b] x sizes[b] blocks (a padded stack
+    makes every eigensolve as large as the largest molecule).  Padding
+    directions get eigenvalue +inf-like 1e300 and unit eigenvectors, after the
+    real ones, so ascending order and occupations are those of the padded
+    solve."""
+    B, n = A.shape[0], A.shape[-1]
+    w = torch.full((B, n), 1e300, dtype=A.dtype, device=A.device)
+    V = torch.eye(n, dtype=A.dtype, device=A.device).repeat(B, 1, 1)
+    sizes = np.asarray(sizes)
+    for s in np.unique(sizes):
+        idx = torch.as_tensor(np.flatnonzero(sizes == s), device=A.device)
+        ws, vs = torch.linalg.eigh(A[idx][:, :s, :s])
+        w[idx, :s] = ws
+        blk = V[idx]
+        blk[:, :s, :s] = vs
+        V[idx] = blk
+    return w, V
+
+
+def _occupied_projector(A, sizes, nocc, max_iter=120, tol=1e-12):
+    """P[b] = projector onto the nocc[b] lowest eigenvectors of the leading
+    sizes[b] x sizes[b] block of A[b] (zero outside it), by canonical
+    purification (Palser and Manolopoulos, Phys. Rev. B 58, 12704 (1998)):
+    batched GEMMs per molecule size instead of eigensolves.  Start from the
+    Gershgorin-scaled P0 = lam/n (mu - A) + N/n with trace N; each step
+    P <- ((1+c) P^2 - P^3)/c (c >= 1/2) or ((1-2c) P + (1+c) P^2 - P^3)/(1-c),
+    c = tr(P^2 - P^3)/tr(P - P^2), until P^2 = P.  Molecules whose P is not
+    idempotent with trace N to tol after max_iter steps (no gap at the Fermi
+    level) are diagonalised instead."""
+    B, n = A.shape[0], A.shape[-1]
+    dev, dt = A.device, A.dtype
+    P = torch.zeros_like(A)
+    sizes = np.asarray(sizes)
+    nocc = torch.as_tensor(np.asarray(nocc), dtype=dt, device=dev)
+    for s in np.unique(sizes):
+        idx = torch.as_tensor(np.flatnonzero(sizes == s), device=dev)
+        F = A[idx][:, :s, :s]
+        N = nocc[idx][:, None, None]
+        eye = torch.eye(s, dtype=dt, device=dev)
+        d = torch.diagonal(F, dim1=1, dim2=2)
+        r = F.abs().sum(-1) - d.abs()
+        emin = (d - r).amin(-1)[:, None, None]
+        emax = (d + r).amax(-1)[:, None, None]
+        mu = d.mean(-1)[:, None, None]
+        lam = torch.minimum(N / (emax - mu), (s - N) / (mu - emin))
+        Q = lam / s * (mu * eye - F) + N / s * eye
+        for it in range(max_iter):
+            Q2 = Q @ Q
+            Q3 = Q2 @ Q
+            trq = torch.diagonal(Q, dim1=1, dim2=2).sum(-1)
+            trq2 = torch.diagonal(Q2, dim1=1, dim2=2).sum(-1)
+            trq3 = torch.diagonal(Q3, dim1=1, dim2=2).sum(-1)
+            den = trq - trq2
+            # near convergence tr(P - P^2) -> 0: McWeeny steps (c = 1/2) there
+            ok = den.abs() > 1e-10
+            c = torch.where(ok, (trq2 - trq3) / torch.where(ok, den, torch.ones_like(den)),
+                            torch.full_like(den, .5))[:, None, None]
+            hi = ((1 + c) * Q2 - Q3) / c
+            lo = ((1 - 2 * c) * Q + (1 + c) * Q2 - Q3) / (1 - c)
+            Q = torch.where(c >= .5, hi, lo)
+            if it % 10 == 9 and float((Q2 - Q).abs().amax()) < tol:
+                break
+        bad = ((Q @ Q - Q).abs().amax((1, 2)) > 100 * tol) | \
+              ((torch.diagonal(Q, dim1=1, dim2=2).sum(-1) - N[:, 0, 0]).abs() > 1e-8)
+        if bool(bad.any()):
+            sel = torch.nonzero(bad).ravel()
+            w, V = torch.linalg.eigh(F[sel])
+            occ = (torch.arange(s, device=dev)[None, :] < N[sel, 0, :]).to(dt)
+            Q[sel] = (V * occ[:, None, :]) @ V.transpose(1, 2)
+        blk = P[idx]
+        blk[:, :s, :s] = Q
+        P[idx] = blk
+    return P
 
 
 class BatchedVHFOpt:
@@ -80,15 +181,8 @@ class BatchedVHFOpt:
         groups = np.unique(key)
         gid = np.searchsorted(groups, key)
         shells_of = [np.flatnonzero(gid == g) for g in range(len(groups))]
-        pair_lists = []
-        for p in range(len(groups)):
-            for q in range(p + 1):
-                i = np.repeat(shells_of[p], len(shells_of[q]))
-                j = np.tile(shells_of[q], len(shells_of[p]))
-                m = self.shell_mol[i] == self.shell_mol[j]
-                if p == q:
-                    m &= i >= j
-                pair_lists.append((i[m], j[m]))
+        pair_lists = [_intra_pairs(shells_of[p], shells_of[q], self.shell_mol, len(self.mols), p == q)
+                      for p in range(len(groups)) for q in range(p + 1)]
         ncp = len(pair_lists)
         locs = np.append(0, np.cumsum([len(x[0]) for x in pair_lists])).astype(np.int32)
         p2s = np.vstack([np.hstack([x[0] for x in pair_lists]),
@@ -174,7 +268,8 @@ class BatchedVHFOpt:
 
 class BatchedRHF:
     """RHF of many molecules in lock step: one batched J/K build per cycle,
-    padded batched DIIS / eigensolver; SAD guess; incremental Fock builds.
+    padded batched DIIS, density by purification; SAD guess; incremental
+    Fock builds.
     Converged molecules keep their Fock matrix (their density no longer
     changes, so the difference density screens their quartets out)."""
 
@@ -225,11 +320,10 @@ class BatchedRHF:
         pad = torch.zeros((B, nmax), dtype=torch.bool, device=dev)
         for b in range(B):
             pad[b, n0[b]:] = True
-        X = torch.zeros_like(S)
-        for b in range(B):
-            w, U = torch.linalg.eigh(S[b, :n0[b], :n0[b]])
-            X[b, :n0[b], :n0[b]] = U * torch.where(w > 1e-12, 1. / torch.sqrt(w.clamp_min(1e-300)), 0.)
-        nocc = torch.tensor([m.nelectron // 2 for m in mols], device=dev)
+        w, U = _eigh_by_size(S, n0)
+        real = torch.arange(nmax, device=dev)[None, :] < torch.as_tensor(n0, device=dev)[:, None]
+        X = U * torch.where(real & (w > 1e-12), 1. / torch.sqrt(w.clamp_min(1e-300)), 0.)[:, None, :]
+        nocc_np = np.array([m.nelectron // 2 for m in mols])
         # gather indices of the diagonal blocks of the block-diagonal matrix
         rows, cols, bid, ri, ci = [], [], [], [], []
         for b in range(B):
@@ -294,12 +388,18 @@ class BatchedRHF:
                 Fd = torch.einsum('bk,kbij->bij', cvec, torch.stack(focks))
             else:
                 Fd = F
-            Fo = X.transpose(1, 2) @ Fd @ X + big_diag
-            mo_e, mo_c = torch.linalg.eigh(Fo)
-            mo_c = X @ mo_c
-            occ = (torch.arange(nmax, device=dev)[None, :] < nocc[:, None]).double()
-            Dn = 2 * (mo_c * occ[:, None, :]) @ mo_c.transpose(1, 2)
-            Dn = torch.where(done[:, None, None], D, Dn)
+            # converged molecules keep their density: only the others are
+            # diagonalised
+            act_np = np.flatnonzero(~done.cpu().numpy())
+            act = torch.as_tensor(act_np, device=dev)
+            Xa = X[act]
+            Fo = Xa.transpose(1, 2) @ Fd[act] @ Xa + big_diag[act]
+            # density from the occupied projector of the orthogonalised Fock
+            # matrix (purification: batched GEMMs; an eigensolve where it
+            # does not converge), D = 2 X P X^T
+            Po = _occupied_projector(Fo, n0[act_np], nocc_np[act_np])
+            Dn = D.clone()
+            Dn[act] = 2 * Xa @ Po @ Xa.transpose(1, 2)
             tj = time.perf_counter()
             dvj, dvk = jk(Dn - D)
             torch.cuda.synchronize()

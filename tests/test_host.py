@@ -310,3 +310,85 @@ def test_host_diis_matches_full_solve():
         ref = np.einsum('i,ijk->jk', c, np.array(fs))
         assert np.abs(got - ref).max() < 1e-10 * max(1., np.abs(ref).max())
         assert np.abs(diis.gram - es @ es.T).max() < 1e-10 * np.abs(es @ es.T).max()
+
+
+def test_batched_intra_pairs_match_masked_product():
+    """The per-molecule pair generation of the batched basis gives the same
+    pairs, in the same order, as the full cross product masked to pairs of
+    one molecule."""
+    from byteqc_b200.scf import batched
+    from byteqc_b200.gto import mole as gto
+    mols = batched.batch_systems(24, seed=3)
+    o = batched.BatchedVHFOpt(mols)
+    key = o.mol._bas[:, gto.ANG_OF] * 1000 + o.mol._bas[:, gto.NPRIM_OF]
+    gid = np.searchsorted(np.unique(key), key)
+    shells_of = [np.flatnonzero(gid == g) for g in range(gid.max() + 1)]
+    for p in range(len(shells_of)):
+        for q in range(p + 1):
+            i = np.repeat(shells_of[p], len(shells_of[q]))
+            j = np.tile(shells_of[q], len(shells_of[p]))
+            m = o.shell_mol[i] == o.shell_mol[j]
+            if p == q:
+                m &= i >= j
+            gi, gj = batched._intra_pairs(shells_of[p], shells_of[q], o.shell_mol, len(mols), p == q)
+            assert np.array_equal(gi, i[m]) and np.array_equal(gj, j[m])
+
+
+def test_batched_eigh_by_size_matches_padded_solve():
+    """Densities from the size-by-size eigensolve of a padded stack equal
+    those of the padded solve with a large diagonal on the padding."""
+    import torch
+    from byteqc_b200.scf.batched import _eigh_by_size
+    rng = np.random.default_rng(2)
+    sizes = np.array([5, 9, 5, 12, 9])
+    B, n = len(sizes), 12
+    A = torch.zeros((B, n, n), dtype=torch.float64)
+    for b, s in enumerate(sizes):
+        m = rng.normal(size=(s, s))
+        A[b, :s, :s] = torch.as_tensor(m + m.T)
+    pad = torch.arange(n)[None, :] >= torch.as_tensor(sizes)[:, None]
+    w0, v0 = torch.linalg.eigh(A + 1e6 * torch.diag_embed(pad.double()))
+    w1, v1 = _eigh_by_size(A, sizes)
+    for b, s in enumerate(sizes):
+        assert torch.allclose(w1[b, :s], w0[b, :s], atol=1e-10)
+        nocc = s // 2
+        d0 = v0[b, :, :nocc] @ v0[b, :, :nocc].T
+        d1 = v1[b, :, :nocc] @ v1[b, :, :nocc].T
+        assert torch.allclose(d0, d1, atol=1e-10)
+
+
+def test_batched_occupied_projector():
+    """Canonical purification gives the projector onto the nocc lowest
+    eigenvectors (against eigh) for gapped spectra of several sizes, one with
+    a far-out eigenvalue like the one given to dropped directions; a spectrum
+    without a gap at the Fermi level falls back to the eigensolver and still
+    returns an idempotent projector of trace nocc."""
+    import torch
+    from byteqc_b200.scf.batched import _occupied_projector
+    rng = np.random.default_rng(7)
+    sizes = np.array([10, 30, 30, 18])
+    n = 30
+    A = torch.zeros((len(sizes), n, n), dtype=torch.float64)
+    nocc = []
+    for b, s in enumerate(sizes):
+        no = s // 3
+        ev = np.r_[-np.sort(rng.uniform(0.3, 20., no))[::-1], rng.uniform(0.1, 8., s - no)]
+        if b == 2:
+            ev[-1] = 1e6
+        if b == 3:
+            ev[no] = ev[no - 1]      # degenerate HOMO/LUMO
+        Q, _ = np.linalg.qr(rng.normal(size=(s, s)))
+        A[b, :s, :s] = torch.as_tensor(Q @ np.diag(ev) @ Q.T)
+        nocc.append(no)
+    P = _occupied_projector(A, sizes, nocc)
+    for b, s in enumerate(sizes):
+        Pb = P[b, :s, :s]
+        assert float((Pb @ Pb - Pb).abs().max()) < 1e-10
+        assert abs(float(Pb.trace()) - nocc[b]) < 1e-8
+        outside = P[b].clone()
+        outside[:s, :s] = 0
+        assert float(outside.abs().max()) == 0.
+        if b < 3:
+            w, V = torch.linalg.eigh(A[b, :s, :s])
+            Pe = V[:, :nocc[b]] @ V[:, :nocc[b]].T
+            assert float((Pb - Pe).abs().max()) < 1e-10
