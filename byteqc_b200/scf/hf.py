@@ -840,7 +840,7 @@ class RHF(_SCFBase):
         h2d = d2h = 0
         diis = HostDIIS(self.diis_space)
         e_last = None
-        vj = vk = dm_last = None
+        vj = vk = dm_last = co = None
         self.converged = False
         mixed = self.fp32_threshold > 0
         final = not mixed
@@ -871,17 +871,23 @@ class RHF(_SCFBase):
                 final = True
             e_last = e
             # F D S - S D F = X - X^T with X = F D S (F, D, S symmetric), as
-            # pyscf forms the DIIS error
-            X = F @ dm @ S
+            # pyscf forms the DIIS error; once D = 2 Co Co^T (after the first
+            # diagonalisation) X = 2 (F Co)(S Co)^T, nocc columns wide
+            if co is None:
+                X = F @ dm @ S
+            else:
+                X = 2. * (F @ co) @ (S @ co).T
             Fd = diis.update(F, X - X.T)
             mo_e, mo_c = self._eigh(Fd, S)
             mo_e = mo_e.cpu().numpy()
             mo_c = mo_c.cpu().numpy()
-            h2d += Fd.nbytes + S.nbytes
+            # S crosses once: its orthogonalizer is kept on the device
+            h2d += Fd.nbytes + (S.nbytes if cycle == 0 else 0)
             d2h += mo_e.nbytes + mo_c.nbytes
             idx = np.argsort(mo_e)[:nocc]
             dm_last = dm
-            dm = 2. * mo_c[:, idx] @ mo_c[:, idx].T
+            co = np.ascontiguousarray(mo_c[:, idx])
+            dm = 2. * co @ co.T
         self.e_tot = e
         self.host_bytes = (h2d, d2h)
         self.timings['total'] = time.perf_counter() - t0
