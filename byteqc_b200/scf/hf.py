@@ -679,7 +679,12 @@ class HostDIIS:
         B[:n, :n] = g
         rhs = np.zeros(n + 1)
         rhs[n] = -1
-        c = np.linalg.solve(B, rhs)[:n]
+        try:
+            c = np.linalg.solve(B, rhs)[:n]
+        except np.linalg.LinAlgError:
+            # singular system (repeated error vectors): no extrapolation,
+            # as the device DIIS does
+            return F
         Fd = self.focks[0] * c[0]
         for ci, Fi in zip(c[1:], self.focks[1:]):
             Fd += ci * Fi
