@@ -20,7 +20,7 @@ import torch
 
 from .. import lib as _libmod
 from ..gto import mole as gto
-from .hf import (_VHFOpt, _dev, _ptr, _stream, basis_seg_contraction, _tile_order, PAIR_TILE,
+from .hf import (_VHFOpt, _dev, _ptr, _stream, basis_seg_contraction, PAIR_TILE,
                  free_basis_cache, make_plan)
 from .guess import atomic_density
 
@@ -44,6 +44,35 @@ def _intra_pairs(sp, sq, shell_mol, nmol, diag):
         keep = i >= j
         i, j = i[keep], j[keep]
     return i, j
+
+
+def _tile_order_mols(bra, ket, q, mol):
+    """The 'q' tile layout of _tile_order applied to each molecule's pairs of
+    one class, for all molecules at once: per molecule (ascending) the pairs
+    sorted by q descending (stably), the run padded to a multiple of
+    PAIR_TILE with copies of its last pair (q = 0, flagged), so no tile mixes
+    molecules.  Returns (bra, ket, q, is_padding, molecule) per slot."""
+    n = len(q)
+    if n == 0:
+        z = np.zeros(0, np.int64)
+        return bra[z], ket[z], q[z], np.zeros(0, bool), np.zeros(0, np.int32)
+    o = np.lexsort((-q, mol))
+    bra, ket, q, mol = bra[o], ket[o], q[o], mol[o]
+    uniq, cnt = np.unique(mol, return_counts=True)
+    pad = (-cnt) % PAIR_TILE
+    tot = cnt + pad
+    ostart = np.r_[0, np.cumsum(tot)[:-1]]
+    istart = np.r_[0, np.cumsum(cnt)[:-1]]
+    src = np.empty(int(tot.sum()), np.int64)
+    is_pad = np.zeros(len(src), bool)
+    g = np.repeat(np.arange(len(uniq)), cnt)
+    src[ostart[g] + np.arange(n) - istart[g]] = np.arange(n)
+    pg = np.repeat(np.arange(len(uniq)), pad)
+    ppos = ostart[pg] + cnt[pg] + np.arange(len(pg)) - np.r_[0, np.cumsum(pad)[:-1]][pg]
+    src[ppos] = istart[pg] + cnt[pg] - 1
+    is_pad[ppos] = True
+    return (bra[src], ket[src], np.where(is_pad, 0., q[src]), is_pad,
+            np.repeat(uniq, tot).astype(np.int32))
 
 
 def _eigh_by_size(A, sizes):
@@ -131,6 +160,7 @@ class BatchedVHFOpt:
         self.mols = mols
         self.direct_scf_tol = cutoff
         parts = [basis_seg_contraction(m) for m in mols]
+        self.parts = parts     # per molecule (decontracted molecule, coeff), unsorted
         self.coeffs = [c for _, c in parts]
         # concatenate the Cartesian molecules (pointer offsets into one env)
         atm, bas, env = [], [], [np.zeros(gto.PTR_ENV_START)]
@@ -206,16 +236,13 @@ class BatchedVHFOpt:
             b, k, q = p2s[0, sl], p2s[1, sl], q_all[sl]
             keepm = q > self.direct_scf_tol
             b, k, q = b[keepm], k[keepm], q[keepm]
-            mb = self.shell_mol[b]
-            for m in np.unique(mb):
-                s = mb == m
-                tb, tk, tq, td = _tile_order(b[s], k[s], q[s])
-                b_all.append(tb)
-                k_all.append(tk)
-                q_out.append(tq)
-                dummies.append(td)
-                mol_out.append(np.full(len(tb), m, dtype=np.int32))
-            new_locs.append(new_locs[-1] + sum(len(x) for x in b_all[len(mol_out) - len(np.unique(mb)):]))
+            tb, tk, tq, td, tm = _tile_order_mols(b, k, q, self.shell_mol[b])
+            b_all.append(tb)
+            k_all.append(tk)
+            q_out.append(tq)
+            dummies.append(td)
+            mol_out.append(tm)
+            new_locs.append(new_locs[-1] + len(tb))
         self.bas_pairs_locs = np.asarray(new_locs, dtype=np.int32)
         cat = lambda x, dt: np.hstack(x).astype(dt) if x else np.zeros(0, dt)
         self.bas_pair2shls = np.vstack([cat(b_all, np.int32), cat(k_all, np.int32)])
@@ -302,7 +329,7 @@ class BatchedRHF:
         e_nuc = torch.tensor([m.energy_nuc() for m in mols], dtype=torch.float64, device=dev)
         for b, m in enumerate(mols):
             single = _VHFOpt.__new__(_VHFOpt)
-            single.mol, single.coeff = basis_seg_contraction(m)
+            single.mol, single.coeff = opt.parts[b]
             single.coeff_dev = torch.as_tensor(single.coeff, device=dev)
             single.nao_cart = single.coeff.shape[0]
             single._mem = {'ao_loc': torch.as_tensor(single.mol.ao_loc_nr(cart=True),

@@ -392,3 +392,27 @@ def test_batched_occupied_projector():
             w, V = torch.linalg.eigh(A[b, :s, :s])
             Pe = V[:, :nocc[b]] @ V[:, :nocc[b]].T
             assert float((Pb - Pe).abs().max()) < 1e-10
+
+
+def test_batched_tile_order_matches_per_molecule_loop():
+    """The all-molecule tile ordering of the batched lists equals the 'q'
+    layout of _tile_order applied molecule by molecule (ties in q included)."""
+    from byteqc_b200.scf import batched
+    from byteqc_b200.scf.hf import _tile_order
+    rng = np.random.default_rng(11)
+    nmol, n = 9, 700
+    mol = np.sort(rng.integers(0, nmol, n)).astype(np.int32)
+    mol[rng.permutation(n)[:50]] = mol[rng.permutation(n)[:50]]   # not sorted by molecule
+    bra = rng.integers(0, 10 ** 5, n).astype(np.int32)
+    ket = rng.integers(0, 10 ** 5, n).astype(np.int32)
+    q = np.round(rng.random(n) * 20) / 20 + 1e-3                    # many ties
+    parts = [[], [], [], [], []]
+    for m in np.unique(mol):
+        s = mol == m
+        tb, tk, tq, td = _tile_order(bra[s], ket[s], q[s])
+        for lst, v in zip(parts, (tb, tk, tq, td, np.full(len(tb), m, np.int32))):
+            lst.append(v)
+    ref = [np.hstack(x) for x in parts]
+    got = batched._tile_order_mols(bra, ket, q, mol)
+    for a, b in zip(got, ref):
+        assert np.array_equal(a, b)
